@@ -1,0 +1,349 @@
+#!/usr/bin/env python
+"""Fused+raycast frames/s at 640x480, 5 mm voxels (plain FP32 single map).
+
+One step = fuse one synthetic RGB-D frame (uint16 mm depth + uint8x3 colour)
+into the map and raycast the vertex + normal maps at that frame's pose,
+through the library's C ABI (libvmap_b200.so).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+N > 1 is launched with torch.distributed.run: every rank maps its own seeded
+scene (independent maps, no collective on the data path: weak scaling) and
+the timed region is the max over ranks of the summed per-step device times.
+--impl reference times the reference algorithm's CPU restatement (the
+reference is CUDA/Eigen/OpenCV code that cannot be built here) on the host
+cores, rank 0 only.
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "fused+raycast frames/s @640x480, 5mm voxels: batched vs plain B200; p99 ms"
+WORKLOAD = "room_full"
+FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=10)
+    p.add_argument("--impl", default="product", choices=["product", "reference"])
+    p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    return p.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def percentile(xs, q):
+    return float(np.percentile(np.asarray(xs, np.float64), q)) if xs else 0.0
+
+
+def workload_config(wl, args, extra=None):
+    cfg = {"workload": "%s: %dx%d depth (uint16 mm) + rgb, %g mm voxels, 2^%d entries, 2^%d-block pool, "
+                       "%s TSDF + weight + uint8x3 colour, figure-8 trajectory; step = fuse one frame + raycast "
+                       "vertex/normal maps at its pose" % (wl.name, wl.width, wl.height, wl.voxel_size * 1e3,
+                                                           int(np.log2(wl.num_entries)), int(np.log2(wl.num_blocks)),
+                                                           wl.voxel_format.upper()),
+           "path": "plain single map per GPU", "frames": "%d..%d" % (args.warmup, args.warmup + args.steps - 1),
+           "warmup_frames": "0..%d" % (args.warmup - 1), "l2": "flushed between steps (256 MiB write)",
+           "parallelism": "independent maps per rank" if args.gpus > 1 else "single GPU"}
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
+              "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+
+    def __init__(self, gpu_id):
+        self.gpu_id = gpu_id
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            cmd = ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits", "-lms",
+                   "200"]
+            if self.gpu_id is not None:
+                cmd += ["-i", str(self.gpu_id)]
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = [r.split(", ") for r in getattr(self, "out", "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def gpu_index(local_rank):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+    if vis:
+        ids = [v.strip() for v in vis.split(",") if v.strip()]
+        if local_rank < len(ids):
+            return ids[local_rank]
+    return local_rank
+
+
+# -------------------------------------------------------------- CPU baseline
+def cpu_oracle_run(wl, frames, n_threads, seconds=None, steps=None):
+    """Reference algorithm (FP32 restatement, same voxel format) on the host:
+    fuse + raycast per frame. Returns per-frame seconds."""
+    from oracle import oracle as O
+    from voxelmapping_b200 import synth
+    O.set_threads(n_threads)
+    om = O.OracleMap(wl.width, wl.height, wl.K, wl.num_blocks, wl.voxel_size, storage=wl.voxel_format,
+                     max_weight=wl.max_weight, with_color=wl.with_color)
+    times = []
+    t_start = time.perf_counter()
+    for i, (d, rgb, pose) in enumerate(frames):
+        t0 = time.perf_counter()
+        om.fuse(synth.depth_to_metres(d, wl.depth_scale), rgb if wl.with_color else None, pose)
+        om.raycast(pose)
+        times.append(time.perf_counter() - t0)
+        if seconds is not None and time.perf_counter() - t_start > seconds:
+            break
+        if steps is not None and len(times) >= steps:
+            break
+    return times
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from voxelmapping_b200 import synth
+    wl = synth.WORKLOADS[WORKLOAD]
+    scene = synth.Scene(wl)
+    frames = [scene.render(i) for i in range(args.warmup + args.steps)]
+    threads = os.cpu_count() or 1
+    times = cpu_oracle_run(wl, frames, threads)
+    timed = times[args.warmup:]
+    total = sum(timed)
+    value = len(timed) / total
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(timed),
+            "p50_ms": 1e3 * percentile(timed, 50), "p99_ms": 1e3 * percentile(timed, 99),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.voxel_format,
+            "data": "synthetic",
+            "config": workload_config(wl, args, {"path": "reference algorithm, CPU restatement (oracle port)"}),
+            "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
+                             "sample": "frames %d..%d of %s, fuse + raycast each (every step a full frame)"
+                                       % (args.warmup, args.warmup + args.steps - 1, WORKLOAD)},
+            "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------- product arm
+def run_product(args):
+    import torch
+    import torch.distributed as dist
+    from voxelmapping_b200 import VoxelMapping
+    from voxelmapping_b200 import _lib as L
+    from voxelmapping_b200 import synth
+
+    rank, world, local = dist_env()
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    wl = synth.WORKLOADS[WORKLOAD]
+    import dataclasses
+    wl_r = dataclasses.replace(wl, seed=wl.seed + rank)
+    scene = synth.Scene(wl_r)
+    nfr = args.warmup + args.steps
+    frames = [scene.render(i) for i in range(nfr)]
+    depth_d = torch.from_numpy(np.stack([f[0] for f in frames]).view(np.int16)).to(dev)
+    rgb_d = torch.from_numpy(np.stack([f[1] for f in frames])).to(dev).reshape(nfr, wl.height, wl.width * 3)
+    poses = [L.pose_arg(f[2]) for f in frames]
+    vm = VoxelMapping(wl.width, wl.height, wl.K, voxel_format=wl.voxel_format, with_color=wl.with_color,
+                      max_weight=wl.max_weight)
+    vm.CreateMap(wl.num_entries, wl.num_blocks, wl.voxel_size)
+    lib = L.lib()
+    vmap = torch.empty((wl.height, wl.width, 4), dtype=torch.float32, device=dev)
+    nmap = torch.empty_like(vmap)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream()
+    sp = C.c_void_p(stream.cuda_stream)
+    counters = torch.zeros((args.steps, 16), dtype=torch.int32, device=dev)
+    h = vm._map
+    vpitch = wl.width * 16
+
+    def step(i):
+        L.check(lib.vmap_fuse_depth_rgb(h, depth_d[i].data_ptr(), L.DEPTH_U16, wl.width * 2, wl.depth_scale,
+                                        rgb_d[i].data_ptr(), wl.width * 3, poses[i], sp))
+        L.check(lib.vmap_render_scene(h, poses[i], vmap.data_ptr(), vpitch, nmap.data_ptr(), vpitch, sp))
+
+    for i in range(args.warmup):
+        step(i)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    L.check(lib.vmap_timing_enable(h, args.steps * 8))
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    with ClockSampler(gpu_index(local)) as clk:
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            ev[k][0].record()
+            step(args.warmup + k)
+            ev[k][1].record()
+            L.check(lib.vmap_copy_counters(h, counters[k].data_ptr(), sp))
+        torch.cuda.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    stage_ms = (C.c_double * 7)()
+    stage_n = (C.c_uint32 * 7)()
+    L.check(lib.vmap_timing_read(h, stage_ms, stage_n))
+    L.check(lib.vmap_timing_enable(h, 0))
+    total_ms = sum(step_ms)
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dist.barrier()
+    max_total_ms = float(t.item())
+    value = world * args.steps / (max_total_ms / 1e3)
+    st = vm.stats()
+    cnt = counters.cpu().numpy()
+    vis = cnt[:, 1].astype(np.float64)
+    alloc = np.minimum(cnt[:, 0], wl.num_blocks).astype(np.float64)
+
+    # --- roofline: algorithmic bytes per launch of each stage (bench model) --
+    P = wl.width * wl.height
+    s_vox = L.lib().vmap_block_bytes(L.FORMAT_NAMES[wl.voxel_format], int(wl.with_color)) / 512.0
+    s_tsdf = {"ref": 3, "f32": 8, "f16": 4, "i16": 4}[wl.voxel_format]
+    stage_bytes = {
+        "alloc": P * 2 + vis.mean() * 32,                         # depth read + one probe sector per block
+        "visibility": alloc.mean() * 8 + vis.mean() * 4,          # block keys + visible list
+        "fuse": vis.mean() * (512 * s_vox * 2 + 12) + P * 5,      # block RMW + depth/colour images
+        "zrange": alloc.mean() * 8,
+        "raycast": vis.mean() * 512 * s_tsdf + P * 16,            # touched blocks' tsdf+weight + vertex map
+        "normals": P * 32,
+    }
+    stages = {}
+    for i, name in enumerate(L.STAGES):
+        if stage_n[i]:
+            per = stage_ms[i] / stage_n[i]
+            b = stage_bytes.get(name)
+            stages[name] = {"launches": int(stage_n[i]), "ms_per_launch": per,
+                            "share": stage_ms[i] / max(sum(stage_ms), 1e-9),
+                            "alg_bytes": b, "gbs": (b / (per * 1e-3) / 1e9) if b else None}
+    dom = max(stages, key=lambda k: stages[k]["ms_per_launch"] * stages[k]["launches"])
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = peaks.get("hbm_gbs")
+    peak_src = "measured" if peak else "fallback"
+    peak = peak or 6650.0
+    traffic = None
+    tf = ROOT / "profiles" / "ncu_traffic.json"
+    if tf.exists():
+        traffic = json.loads(tf.read_text()).get(dom, {}).get("dram_bytes_per_launch")
+    roof = {"kernel": dom, "bound": "hbm", "achieved": stages[dom]["gbs"], "peak": peak, "peak_source": peak_src,
+            "unit": "GB/s", "frac": stages[dom]["gbs"] / peak, "traffic": traffic,
+            "alg_bytes_per_launch": stages[dom]["alg_bytes"]}
+
+    line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_total_ms / args.steps,
+            "p50_ms": percentile(step_ms, 50), "p99_ms": percentile(step_ms, 99), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": wl.voxel_format, "data": "synthetic",
+            "config": workload_config(wl, args), "roofline": roof, "stages": stages,
+            "gpu_launches": int(sum(stage_n)), "clocks": clk.summary(),
+            "map": {"allocated_blocks": int(st["allocated_blocks"]), "visible_blocks_mean": float(vis.mean()),
+                    "error_flags": int(st["error_flags"])}}
+
+    # --- e2e: same steps through the host-buffer C ABI calls --------------
+    if not args.no_e2e:
+        depth_h = torch.from_numpy(np.stack([f[0] for f in frames]).view(np.int16)).pin_memory()
+        rgb_h = torch.from_numpy(np.stack([f[1] for f in frames])).pin_memory()
+        vmap_h = torch.empty((wl.height, wl.width, 4), dtype=torch.float32).pin_memory()
+        nmap_h = torch.empty_like(vmap_h).pin_memory()
+        vm.reset()
+
+        def step_host(i):
+            L.check(lib.vmap_fuse_host(h, depth_h[i].data_ptr(), L.DEPTH_U16, wl.depth_scale, rgb_h[i].data_ptr(),
+                                       poses[i], sp))
+            L.check(lib.vmap_render_scene_host(h, poses[i], vmap_h.data_ptr(), nmap_h.data_ptr(), sp))
+
+        for i in range(args.warmup):
+            step_host(i)
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+        for k in range(args.steps):
+            flush.fill_(k & 255)
+            ev2[k][0].record()
+            step_host(args.warmup + k)
+            ev2[k][1].record()
+        torch.cuda.synchronize()
+        e_ms = [a.elapsed_time(b) for a, b in ev2]
+        t2 = torch.tensor([sum(e_ms)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        line["e2e"] = {"value": world * args.steps / (float(t2.item()) / 1e3), "unit": "frames/s",
+                       "h2d_bytes_per_step": P * 2 + P * 3, "d2h_bytes_per_step": 2 * P * 16,
+                       "p50_ms": percentile(e_ms, 50), "p99_ms": percentile(e_ms, 99),
+                       "path": "vmap_fuse_host + vmap_render_scene_host, pinned host buffers"}
+
+    # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        times = cpu_oracle_run(wl, frames, threads, seconds=args.cpu_seconds)
+        line["cpu_baseline"] = {"value": len(times) / sum(times), "unit": "frames/s", "cores": threads,
+                                "kind": "port",
+                                "sample": "frames 0..%d of %s (fuse + raycast each, FP32 reference-algorithm "
+                                          "restatement, %d threads)" % (len(times) - 1, WORKLOAD, threads)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    vm.release()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_product(args)
+
+
+if __name__ == "__main__":
+    main()

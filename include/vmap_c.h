@@ -1,0 +1,220 @@
+/*
+ * vmap_c.h - C ABI of the B200 voxel-hashing TSDF library (libvmap_b200.so).
+ *
+ * Drop-in boundary for xingruiyang/VoxelMapping. The reference exposes a C++
+ * pimpl class (include/vmapping.h:10-27) over templated CUDA launchers
+ * (src/device_functions.h:11-66); this header flattens that surface into plain
+ * functions over an opaque map handle so any FFI (ctypes, cgo, JNI, N-API) can
+ * bind it. include/vmapping.h (this repository) rebuilds the reference's class
+ * on top of these functions.
+ *
+ * Conventions
+ *  - Poses are camera-to-world, row-major 4x4 doubles; the library composes and
+ *    inverts them in FP64 and hands FP32 copies to the kernels.
+ *  - Device pointers (`_dev`) must be CUDA device memory; `_host` pointers host
+ *    memory (pinned for asynchronous copies). Pitches are in bytes.
+ *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *    All calls are asynchronous on that stream unless documented otherwise;
+ *    no call synchronises the device or reads counters back to the host
+ *    except vmap_get_stats / vmap_polygonize_host / the *_host variants.
+ *  - Errors: every call returns a vmap_status. Conditions detected on the GPU
+ *    (pool or hash table full, coordinates out of range, mesh buffer full) are
+ *    accumulated as sticky flags read by vmap_get_stats. Nothing calls exit().
+ *  - Not thread-safe per map; distinct maps may be driven from distinct
+ *    threads and streams.
+ */
+#ifndef VMAP_C_H
+#define VMAP_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VMAP_ABI_VERSION 1
+
+typedef enum vmap_status {
+    VMAP_OK = 0,
+    VMAP_ERR_INVALID_ARG = 1,
+    VMAP_ERR_CUDA = 2,          /* a CUDA runtime call failed (see vmap_last_error) */
+    VMAP_ERR_OUT_OF_MEMORY = 3, /* device or host allocation failed              */
+    VMAP_ERR_POOL_FULL = 4,     /* voxel-block pool exhausted                    */
+    VMAP_ERR_HASH_FULL = 5,     /* probe limit reached in the block hash table   */
+    VMAP_ERR_RANGE = 6,         /* block coordinate outside +-2^20               */
+    VMAP_ERR_BUFFER_FULL = 7,   /* mesh output buffer too small                  */
+    VMAP_ERR_NO_DEVICE = 8      /* no CUDA device / wrong architecture           */
+} vmap_status;
+
+/* sticky device-side error flags (vmap_stats.error_flags) */
+#define VMAP_FLAG_POOL_FULL 1u
+#define VMAP_FLAG_HASH_FULL 2u
+#define VMAP_FLAG_RANGE 4u
+#define VMAP_FLAG_BUFFER_FULL 8u
+
+/* Voxel storage formats. REF is the reference's Voxel (int16 TSDF x32767,
+ * uint8 weight, map_struct.h:17-21); F32 is the plain single-precision map;
+ * F16 / I16 are the reduced-precision formats with uint16 weights. */
+typedef enum vmap_voxel_format {
+    VMAP_VOXEL_REF = 0, /* int16 tsdf, uint8 weight   : 3 B/voxel (+3 colour) */
+    VMAP_VOXEL_F32 = 1, /* float tsdf, float weight   : 8 B/voxel (+3 colour) */
+    VMAP_VOXEL_F16 = 2, /* half tsdf, uint16 weight   : 4 B/voxel (+3 colour) */
+    VMAP_VOXEL_I16 = 3  /* int16 tsdf, uint16 weight  : 4 B/voxel (+3 colour) */
+} vmap_voxel_format;
+
+typedef enum vmap_depth_type {
+    VMAP_DEPTH_F32 = 0, /* float metres (reference GpuMat CV_32FC1)        */
+    VMAP_DEPTH_U16 = 1  /* uint16 scaled by depth_scale (e.g. 0.001 = mm)  */
+} vmap_depth_type;
+
+typedef struct vmap_config {
+    /* camera: reference VoxelMapping(int w, int h, const Matrix3f& K) */
+    int width, height;
+    float fx, fy, cx, cy;
+    /* map: reference CreateMap(int numEntries, int numVoxels, float voxelSize) */
+    int num_entries;          /* hash entries requested (>= 0; must fit 4 * num_buckets) */
+    int num_blocks;           /* voxel-block pool capacity ("numVoxels")        */
+    float voxel_size;         /* metres                                         */
+    /* extensions (0 selects the reference default) */
+    int num_buckets;          /* 0: int(0.9 * num_blocks) as the reference       */
+    float truncation;         /* 0: 4 * voxel_size                              */
+    int voxel_format;         /* vmap_voxel_format                              */
+    int max_weight;           /* 0: 255                                         */
+    int with_color;           /* keep uint8x3 colour per voxel                  */
+    int raycast_mode;         /* 0: z-range bounded march (default), 1: full march from 0.1 m */
+} vmap_config;
+
+typedef struct vmap_stats {
+    uint32_t allocated_blocks;  /* blocks in use                                 */
+    uint32_t capacity_blocks;
+    uint32_t visible_blocks;    /* visible blocks of the last fuse (numVisBlock) */
+    uint32_t error_flags;       /* VMAP_FLAG_* (sticky until vmap_clear_errors)  */
+    uint32_t failed_allocs;     /* allocations refused because the pool was full */
+    uint32_t last_triangles;    /* triangles found by the last polygonize (unclamped) */
+    uint64_t pool_bytes;        /* device bytes of the voxel pool                */
+    uint64_t device_bytes;      /* all device bytes owned by the map            */
+} vmap_stats;
+
+typedef struct vmap_map vmap_map;
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* VoxelMapping(w,h,K) + CreateMap (vmapping.cpp:57-75, map_struct.cu:44-66):
+ * allocates the hash table, block pool and work buffers on the current device
+ * and resets them. Synchronous. */
+vmap_status vmap_create(const vmap_config* cfg, vmap_map** out);
+/* ~VoxelMapping / MapStruct::release (map_struct.cu:68-79). Synchronous. */
+vmap_status vmap_destroy(vmap_map* map);
+/* VoxelMapping::reset / MapStruct::reset (map_struct.cu:29-42): empties the
+ * map, keeps the allocations. */
+vmap_status vmap_reset(vmap_map* map, void* stream);
+vmap_status vmap_get_config(const vmap_map* map, vmap_config* out);
+
+/* ---- fusion -------------------------------------------------------------- */
+/* VoxelMapping::FuseDepth (vmapping.cpp:162 -> FuseImage, depth_fusion.cu:199-301):
+ * allocate blocks along each depth ray, select visible blocks, update
+ * TSDF/weight. depth_dev has the map's width x height. */
+vmap_status vmap_fuse_depth(vmap_map* map, const void* depth_dev, int depth_type, size_t depth_pitch,
+                            float depth_scale, const double pose[16], void* stream);
+/* VoxelMapping::FuseDepthAndImage (vmapping.cpp:167, FuseDepthAndImage
+ * depth_fusion.cu:383-488): as above plus colour (uint8x3 per pixel, blended
+ * 0.7 old + 0.3 new). Requires with_color. */
+vmap_status vmap_fuse_depth_rgb(vmap_map* map, const void* depth_dev, int depth_type, size_t depth_pitch,
+                                float depth_scale, const uint8_t* rgb_dev, size_t rgb_pitch,
+                                const double pose[16], void* stream);
+/* Host-buffer variant (the reference's FuseDepthAndImage takes cv::Mat):
+ * copies depth (and rgb, may be NULL) into device staging, then fuses. */
+vmap_status vmap_fuse_host(vmap_map* map, const void* depth_host, int depth_type, float depth_scale,
+                           const uint8_t* rgb_host, const double pose[16], void* stream);
+/* CheckVisibleBlocks (depth_fusion.cu:494-539): visible-block selection at a
+ * pose; count readable through vmap_get_stats. */
+vmap_status vmap_check_visible_blocks(vmap_map* map, const double pose[16], void* stream);
+
+/* ---- raycast ------------------------------------------------------------- */
+/* VoxelMapping::RenderScene (vmapping.cpp:83-104; ProjectRenderingBlocks
+ * ray_tracing.cu:171-234 + RenderScene :403-437) fused with computeNormal
+ * (image_proc.cu:95-104): vertex map (float4, camera frame, w = 1, all-NaN on
+ * a miss) and, if nmap_dev != NULL, normal map (float4, all-NaN where
+ * undefined). */
+vmap_status vmap_render_scene(vmap_map* map, const double pose[16], float* vmap_dev, size_t vmap_pitch,
+                              float* nmap_dev, size_t nmap_pitch, void* stream);
+/* Host-buffer variant: results copied into host buffers (w*h*4 floats each,
+ * nmap_host may be NULL). Asynchronous for pinned memory. */
+vmap_status vmap_render_scene_host(vmap_map* map, const double pose[16], float* vmap_host, float* nmap_host,
+                                   void* stream);
+/* computeNormal (image_proc.h:11, image_proc.cu:74-104) on any float4 map. */
+vmap_status vmap_compute_normal(const float* vmap_dev, size_t vmap_pitch, float* nmap_dev, size_t nmap_pitch,
+                                int width, int height, void* stream);
+/* renderScene (image_proc.h:10, image_proc.cu:8-72): Phong shading of vertex
+ * + normal maps into RGBA8. */
+vmap_status vmap_render_phong(const float* vmap_dev, size_t vmap_pitch, const float* nmap_dev,
+                              size_t nmap_pitch, uint8_t* rgba_dev, size_t rgba_pitch, int width, int height,
+                              void* stream);
+
+/* ---- meshing ------------------------------------------------------------- */
+/* Polygonize (marching_cubes.cu:251-305): marching cubes over all allocated
+ * blocks. Writes at most max_tris triangles (9 floats each for verts and
+ * norms, world metres); the unclamped count goes to *n_tris_dev (device
+ * uint32, may be NULL) and to vmap_stats.last_triangles. */
+vmap_status vmap_polygonize(vmap_map* map, float* verts_dev, float* norms_dev, uint32_t max_tris,
+                            uint32_t* n_tris_dev, void* stream);
+/* VoxelMapping::Polygonize (vmapping.cpp:119-132, 182): mesh into library-owned
+ * device buffers, copied to library-owned host buffers; *verts / *norms point
+ * at them until the next call. Synchronous. Returns the triangle count in
+ * *n_tris (clamped to the buffer). */
+vmap_status vmap_polygonize_host(vmap_map* map, const float** verts, const float** norms, uint32_t* n_tris,
+                                 void* stream);
+/* GetSurfacePoints (marching_cubes.cu:314-344, vmapping.cpp:134-147): triangle
+ * centroids, 3 floats each. */
+vmap_status vmap_surface_points(const float* verts_dev, uint32_t n_tris, float* points_dev, void* stream);
+
+/* ---- inspection ---------------------------------------------------------- */
+/* Synchronises `stream`, then reads the device counters. */
+vmap_status vmap_get_stats(vmap_map* map, void* stream, vmap_stats* out);
+vmap_status vmap_clear_errors(vmap_map* map, void* stream);
+/* Asynchronous copy of the raw device counters (16 x uint32: [0] blocks
+ * handed out, may exceed capacity; [1] visible blocks; [2] error flags;
+ * [3] triangles; [4] refused allocations) to dst (device or pinned host
+ * memory), ordered on `stream`; for monitoring without a synchronisation. */
+vmap_status vmap_copy_counters(vmap_map* map, uint32_t* dst, void* stream);
+/* Dense export of the allocated blocks in pool order (also the snapshot
+ * format): coords int32 x3 per block, tsdf float x512 (dequantised), weight
+ * float x512, rgb uint8 x3x512 (may be NULL). Voxel index x + 8y + 64z.
+ * Buffers are host memory sized for max_blocks. Synchronous. */
+vmap_status vmap_export_blocks(vmap_map* map, int32_t* coords, float* tsdf, float* weight, uint8_t* rgb,
+                               uint32_t max_blocks, uint32_t* n_blocks, void* stream);
+
+/* ---- stage timing (no counterpart in the reference, which has no timers) --
+ * When enabled, every kernel launch of the map is bracketed by CUDA events on
+ * the caller's stream; vmap_timing_read synchronises on them and returns the
+ * summed device time and launch count per stage since the last read. */
+typedef enum vmap_stage {
+    VMAP_STAGE_ALLOC = 0,      /* block allocation along depth rays     */
+    VMAP_STAGE_VISIBILITY = 1, /* visible-block selection               */
+    VMAP_STAGE_FUSE = 2,       /* TSDF / weight / colour update         */
+    VMAP_STAGE_ZRANGE = 3,     /* per-tile depth bounds                 */
+    VMAP_STAGE_RAYCAST = 4,    /* ray marching                          */
+    VMAP_STAGE_NORMALS = 5,    /* normal map                            */
+    VMAP_STAGE_MESH = 6,       /* marching cubes                        */
+    VMAP_NUM_STAGES = 7
+} vmap_stage;
+/* max_records: event pairs to keep (0 disables timing). */
+vmap_status vmap_timing_enable(vmap_map* map, uint32_t max_records);
+vmap_status vmap_timing_read(vmap_map* map, double ms[VMAP_NUM_STAGES], uint32_t launches[VMAP_NUM_STAGES]);
+
+/* ---- utilities ----------------------------------------------------------- */
+/* The library's pose inverse (FP64, affine), exposed for parity tests. */
+void vmap_pose_inverse(const double pose[16], double inv[16]);
+/* hash (map_struct.h:104-109), exposed for parity tests. */
+int vmap_block_hash(int x, int y, int z, int n_buckets);
+/* Bytes per voxel block for a format. */
+size_t vmap_block_bytes(int voxel_format, int with_color);
+const char* vmap_status_string(vmap_status s);
+/* Text of the last CUDA error seen by this thread. */
+const char* vmap_last_error(void);
+int vmap_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VMAP_C_H */

@@ -1,0 +1,94 @@
+"""In-tree build of the native libraries.
+
+* ``libvmap_b200.so``  - the CUDA library behind include/vmap_c.h (sm_100a only)
+* ``libvmap_synth.so`` - the synthetic RGB-D scene generator (host C++)
+
+Run ``python -m voxelmapping_b200.build`` (or ``__graft_entry__.build()``).
+Objects are rebuilt only when a source or header is newer than the output.
+"""
+import concurrent.futures as cf
+import os
+import shutil
+import subprocess
+import sys
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+OBJ = PKG / "_build"
+LIB = PKG / "libvmap_b200.so"
+SYNTH = PKG / "libvmap_synth.so"
+
+CUDA_SOURCES = ["fusion.cu", "raycast.cu", "mesh.cu", "map.cu"]
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",
+                     "--expt-relaxed-constexpr", "-I" + str(ROOT / "include")]
+# host compiler: the system g++ (the one nvcc uses); $CXX may point elsewhere
+HOST_CXX = "/usr/bin/g++" if Path("/usr/bin/g++").exists() else "g++"
+
+
+def nvcc():
+    cand = os.environ.get("CUDA_HOME", "/usr/local/cuda") + "/bin/nvcc"
+    return cand if Path(cand).exists() else (shutil.which("nvcc") or "nvcc")
+
+
+def _headers():
+    return list(CSRC.glob("*.cuh")) + list(CSRC.glob("*.h")) + list(CSRC.glob("*.inc")) + \
+        list((ROOT / "include").glob("*.h"))
+
+
+def _stale(out, deps):
+    if not out.exists():
+        return True
+    t = out.stat().st_mtime
+    return any(Path(d).stat().st_mtime > t for d in deps)
+
+
+def _run(cmd, verbose):
+    if verbose:
+        print(" ".join(str(c) for c in cmd), flush=True)
+    r = subprocess.run([str(c) for c in cmd], capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError("build failed: %s\n%s%s" % (" ".join(map(str, cmd)), r.stdout, r.stderr))
+    if verbose and (r.stdout.strip() or r.stderr.strip()):
+        print(r.stdout + r.stderr, flush=True)
+    return r
+
+
+def build(verbose=False, ptxas_info=False):
+    OBJ.mkdir(exist_ok=True)
+    hdrs = _headers()
+    jobs = []
+    objs = []
+    for src in CUDA_SOURCES:
+        s = CSRC / src
+        o = OBJ / (src + ".o")
+        objs.append(o)
+        if _stale(o, [s] + hdrs):
+            extra = ["-Xptxas", "-v"] if ptxas_info else []
+            jobs.append([nvcc()] + NVCC_FLAGS + extra + ["-c", s, "-o", o])
+    with cf.ThreadPoolExecutor(max_workers=len(CUDA_SOURCES)) as ex:
+        for r in ex.map(lambda c: _run(c, verbose), jobs):
+            if ptxas_info:
+                print(r.stderr)
+    if _stale(LIB, objs):
+        _run([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"],
+             verbose)
+    synth_src = CSRC / "synth.cpp"
+    if _stale(SYNTH, [synth_src, CSRC / "vmap_synth.h"]):
+        _run([HOST_CXX, "-O2", "-std=c++17", "-fPIC", "-fopenmp", "-shared", "-Wall", "-o", SYNTH, synth_src],
+             verbose)
+    return LIB
+
+
+def build_oracle(verbose=False):
+    """Compile the CPU oracle (test infrastructure) with its Makefile."""
+    _run(["make", "-s", "-C", ROOT / "oracle", "CC=" + ("/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc")],
+         verbose)
+    return ROOT / "oracle" / "libvmap_oracle.so"
+
+
+if __name__ == "__main__":
+    build(verbose=True, ptxas_info="--ptxas" in sys.argv)
+    build_oracle(verbose=True)

@@ -1,0 +1,280 @@
+// Fusion path: block allocation along depth rays, visible-block selection and
+// the projective TSDF / weight / colour update.
+//
+// Reference: src/depth_fusion.cu (FuseImage :199-301, FuseDepthAndImage
+// :383-488, CheckVisibleBlocks :494-539) and the device helpers of
+// include/map_struct.h. The reference synchronises the device three times and
+// copies the visible count to the host on every fuse; here the three kernels
+// run back to back on one stream and the counts stay in device memory.
+#include "vmap_launch.h"
+
+namespace vmapb {
+
+template <int DT>
+__device__ __forceinline__ float read_depth(const FrameParams& f, int x, int y)
+{
+    const char* row = reinterpret_cast<const char*>(f.depth) + (size_t)y * f.dpitch;
+    if constexpr (DT == VMAP_DEPTH_F32) {
+        return __ldg(reinterpret_cast<const float*>(row) + x);
+    } else {
+        return __fmul_rn(__uint2float_rn(__ldg(reinterpret_cast<const unsigned short*>(row) + x)), f.dscale);
+    }
+}
+
+// ---------------------------------------------------------------- allocation
+// One thread per depth pixel (CreateBlockLineTracingFunctor,
+// depth_fusion.cu:32-59): the band [d - mu/2, d + mu/2] is unprojected to
+// world voxel coordinates, sampled at ceil(2 |far - near|) points and every
+// sampled block is inserted. Consecutive samples in the same block are
+// inserted once and a warp inserts each distinct block once
+// (__match_any_sync), which leaves the resulting block set unchanged.
+template <int DT>
+__global__ void __launch_bounds__(256) alloc_kernel(DevMap m, FrameParams f)
+{
+    const int lane = threadIdx.x & 31;
+    const int x = blockIdx.x * 32 + lane;
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    int n = 0;
+    float px = 0.f, py = 0.f, pz = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
+    if (x < f.W && y < f.H) {
+        const float d = read_depth<DT>(f, x, y);
+        if (!(isnan(d) || d < kMinDepth || d > kMaxDepth)) {
+            const float tdh = __fmul_rn(m.mu, 0.5f);
+            const float dn = fmaxf(kMinDepth, __fsub_rn(d, tdh));
+            const float df = fmaxf(kMinDepth, __fadd_rn(d, tdh));
+            if (dn < df) {
+                const float3 a = unproject(x, y, dn, f.ifx, f.ify, f.cx, f.cy);
+                const float3 wa = xf_apply(f.T, a.x, a.y, a.z);
+                const float3 b = unproject(x, y, df, f.ifx, f.ify, f.cx, f.cy);
+                const float3 wb = xf_apply(f.T, b.x, b.y, b.z);
+                // worldPtToVoxelPos: (int)floor(p / voxelSize)
+                const int nx = __float2int_rz(floorf(__fdiv_rn(wa.x, m.vs)));
+                const int ny = __float2int_rz(floorf(__fdiv_rn(wa.y, m.vs)));
+                const int nz = __float2int_rz(floorf(__fdiv_rn(wa.z, m.vs)));
+                const int fx = __float2int_rz(floorf(__fdiv_rn(wb.x, m.vs)));
+                const int fy = __float2int_rz(floorf(__fdiv_rn(wb.y, m.vs)));
+                const int fz = __float2int_rz(floorf(__fdiv_rn(wb.z, m.vs)));
+                float3 dir = make_float3(__int2float_rn(fx - nx), __int2float_rn(fy - ny), __int2float_rn(fz - nz));
+                const float len = __fsqrt_rn(sqnorm(dir));
+                // (int)ceil(2.0 * len): the double product of a float by 2 is exact
+                n = __float2int_rz(ceilf(__fmul_rn(2.f, len)));
+                const float den = __int2float_rn(n - 1);
+                dx = __fdiv_rn(dir.x, den);
+                dy = __fdiv_rn(dir.y, den);
+                dz = __fdiv_rn(dir.z, den);
+                px = __int2float_rn(nx);
+                py = __int2float_rn(ny);
+                pz = __int2float_rn(nz);
+            }
+        }
+    }
+    const unsigned full = 0xffffffffu;
+    const int nmax = __reduce_max_sync(full, n);
+    int lbx = INT_MIN, lby = INT_MIN, lbz = INT_MIN;
+    for (int s = 0; s < nmax; ++s) {
+        unsigned long long key = kEmptyKey;
+        int bx = 0, by = 0, bz = 0;
+        if (s < n) {
+            // pt_start.cast<int>() truncates toward zero, then voxelPosToBlockPos
+            bx = vox2blk(__float2int_rz(px));
+            by = vox2blk(__float2int_rz(py));
+            bz = vox2blk(__float2int_rz(pz));
+            if (bx != lbx || by != lby || bz != lbz) {
+                lbx = bx;
+                lby = by;
+                lbz = bz;
+                if (coord_ok(bx, by, bz)) key = pack_key(bx, by, bz);
+                else atomicOr(m.ctr + C_ERR, VMAP_FLAG_RANGE);
+            }
+            px = __fadd_rn(px, dx);
+            py = __fadd_rn(py, dy);
+            pz = __fadd_rn(pz, dz);
+        }
+        const unsigned peers = __match_any_sync(full, key);
+        if (key != kEmptyKey && (__ffs(peers) - 1) == lane) hash_insert(m, bx, by, bz);
+    }
+}
+
+// ---------------------------------------------------------------- visibility
+// CheckEntryVisibilityFunctor (depth_fusion.cu:82-126) without the full
+// hash-table scan: allocated blocks are dense in pool order, so only
+// min(alloc, capacity) 8-byte keys are read. Visible slots are compacted
+// with one atomic per warp.
+__global__ void __launch_bounds__(256) visibility_kernel(DevMap m, FrameParams f)
+{
+    const int n = allocated_blocks(m);
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int nwarps = (gridDim.x * blockDim.x) >> 5;
+    const float scale = __fmul_rn(m.vs, 8.f);
+    for (int base = warp * 32; base < n; base += nwarps * 32) {
+        const int i = base + lane;
+        bool vis = false;
+        if (i < n) {
+            const int3 b = unpack_key(m.blockKeys[i]);
+            vis = block_visible(b.x, b.y, b.z, f.Ti, scale, f.W, f.H, f.fx, f.fy, f.cx, f.cy);
+        }
+        const unsigned mask = __ballot_sync(0xffffffffu, vis);
+        if (mask == 0) continue;
+        unsigned first = 0;
+        if (lane == 0) first = atomicAdd(m.ctr + C_VISIBLE, (unsigned)__popc(mask));
+        first = __shfl_sync(0xffffffffu, first, 0);
+        if (vis) m.visList[first + __popc(mask & ((1u << lane) - 1))] = i;
+    }
+}
+
+// ----------------------------------------------------------------- fusion
+// DepthFusionFunctor / ImageFusionFunctor (depth_fusion.cu:148-196, 328-380).
+// 64 threads per block, one 8-voxel x-row each; 4 blocks per 256-thread CTA,
+// grid-stride over the visible list. A row is read and written (16-byte
+// vector accesses per plane) only when at least one of its voxels updates.
+template <int FMT, bool COLOR, int DT>
+__global__ void __launch_bounds__(256) fuse_kernel(DevMap m, FrameParams f)
+{
+    typedef Layout<FMT> L;
+    typedef typename L::T T;
+    typedef typename L::W W;
+    typedef Fmt<FMT> F;
+    const int team = threadIdx.x >> 6;
+    const int row = threadIdx.x & 63;
+    const int ly = row & 7, lz = row >> 3;
+    const int nvis = m.ctr[C_VISIBLE];
+    const int r0 = lz * 64 + ly * 8;
+    for (int i = blockIdx.x * 4 + team; i < nvis; i += gridDim.x * 4) {
+        const int slot = m.visList[i];
+        const int3 bp = unpack_key(m.blockKeys[slot]);
+        const int vx0 = bp.x * 8;
+        const float wy = __fmul_rn(__int2float_rn(bp.y * 8 + ly), m.vs);
+        const float wz = __fmul_rn(__int2float_rn(bp.z * 8 + lz), m.vs);
+        float sdfv[8];
+        int pu[8], pv[8];
+        unsigned mask = 0;
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+            const float3 p = xf_apply(f.Ti, __fmul_rn(__int2float_rn(vx0 + x), m.vs), wy, wz);
+            // __float2int_rd(fx * p0 / p2 + cx + 0.5)
+            const int u = __float2int_rd(__fadd_rn(__fadd_rn(__fdiv_rn(__fmul_rn(f.fx, p.x), p.z), f.cx), 0.5f));
+            const int v = __float2int_rd(__fadd_rn(__fadd_rn(__fdiv_rn(__fmul_rn(f.fy, p.y), p.z), f.cy), 0.5f));
+            pu[x] = u;
+            pv[x] = v;
+            sdfv[x] = 0.f;
+            if (u < 0 || v < 0 || u > f.W - 1 || v > f.H - 1) continue;
+            const float d = read_depth<DT>(f, u, v);
+            if (isnan(d) || d > kMaxDepth || d < kMinDepth) continue;
+            float sdf = __fsub_rn(d, p.z);
+            if (sdf < -m.mu) continue;
+            sdfv[x] = fminf(1.f, __fdiv_rn(sdf, m.mu));
+            mask |= 1u << x;
+        }
+        if (!mask) continue;
+        unsigned char* blk = m.pool + (size_t)slot * m.blockBytes;
+        T t[8];
+        W w[8];
+        load_row<8 * sizeof(T)>(blk + L::kTsdfOff + r0 * sizeof(T), t);
+        load_row<8 * sizeof(W)>(blk + L::kWOff + r0 * sizeof(W), w);
+        unsigned char c[3][8];
+        if constexpr (COLOR) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) load_row<8>(blk + L::kRgbOff + k * kBlockVoxels + r0, c[k]);
+        }
+#pragma unroll
+        for (int x = 0; x < 8; ++x) {
+            if (!(mask & (1u << x))) continue;
+            const float ow = F::wf(w[x]);
+            const uint8_t* px = nullptr;
+            if constexpr (COLOR) px = f.rgb + (size_t)pv[x] * f.rgbPitch + 3 * pu[x];
+            if (ow == 0.f) {
+                t[x] = F::q(sdfv[x]);
+                w[x] = F::wq(1.f);
+                if constexpr (COLOR) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) c[k][x] = __ldg(px + k);
+                }
+            } else {
+                const float os = F::dq(t[x]);
+                t[x] = F::q(__fdiv_rn(__fmaf_rn(os, ow, sdfv[x]), __fadd_rn(ow, 1.f)));
+                w[x] = F::wq(fminf(__fadd_rn(ow, 1.f), m.wmax));
+                if constexpr (COLOR) {
+#pragma unroll
+                    for (int k = 0; k < 3; ++k)
+                        c[k][x] = (unsigned char)__float2int_rz(
+                            __fmaf_rn(0.7f, __uint2float_rn(c[k][x]), __fmul_rn(0.3f, __uint2float_rn(__ldg(px + k)))));
+                }
+            }
+        }
+        store_row<8 * sizeof(T)>(blk + L::kTsdfOff + r0 * sizeof(T), t);
+        store_row<8 * sizeof(W)>(blk + L::kWOff + r0 * sizeof(W), w);
+        if constexpr (COLOR) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) store_row<8>(blk + L::kRgbOff + k * kBlockVoxels + r0, c[k]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------- reset
+// MapStruct::reset (map_struct.cu:29-42): empty hash slots, pool pointer 0,
+// zeroed voxels.
+__global__ void reset_hash_kernel(DevMap m)
+{
+    const size_t n = (size_t)m.nBucket * kSlots;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        m.keys[i] = kEmptyKey;
+        m.vals[i] = -1;
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+cudaError_t launch_alloc(const DevMap& m, const FrameParams& f, const Launcher&, cudaStream_t s)
+{
+    dim3 grid((f.W + 31) / 32, (f.H + 7) / 8);
+    if (f.dtype == VMAP_DEPTH_U16) alloc_kernel<VMAP_DEPTH_U16><<<grid, 256, 0, s>>>(m, f);
+    else alloc_kernel<VMAP_DEPTH_F32><<<grid, 256, 0, s>>>(m, f);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_visibility(const DevMap& m, const FrameParams& f, const Launcher& l, cudaStream_t s)
+{
+    cudaError_t e = cudaMemsetAsync(m.ctr + C_VISIBLE, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    visibility_kernel<<<l.numSMs * 2, 256, 0, s>>>(m, f);
+    return cudaGetLastError();
+}
+
+template <int FMT, bool COLOR>
+static void fuse_dispatch_dt(const DevMap& m, const FrameParams& f, int grid, cudaStream_t s)
+{
+    if (f.dtype == VMAP_DEPTH_U16) fuse_kernel<FMT, COLOR, VMAP_DEPTH_U16><<<grid, 256, 0, s>>>(m, f);
+    else fuse_kernel<FMT, COLOR, VMAP_DEPTH_F32><<<grid, 256, 0, s>>>(m, f);
+}
+
+template <int FMT>
+static void fuse_dispatch(const DevMap& m, bool color, const FrameParams& f, int grid, cudaStream_t s)
+{
+    if (color) fuse_dispatch_dt<FMT, true>(m, f, grid, s);
+    else fuse_dispatch_dt<FMT, false>(m, f, grid, s);
+}
+
+cudaError_t launch_fuse(const DevMap& m, int fmt, bool color, const FrameParams& f, const Launcher& l,
+                        cudaStream_t s)
+{
+    const int grid = l.numSMs * 8;
+    switch (fmt) {
+    case VMAP_VOXEL_REF: fuse_dispatch<VMAP_VOXEL_REF>(m, color, f, grid, s); break;
+    case VMAP_VOXEL_F32: fuse_dispatch<VMAP_VOXEL_F32>(m, color, f, grid, s); break;
+    case VMAP_VOXEL_F16: fuse_dispatch<VMAP_VOXEL_F16>(m, color, f, grid, s); break;
+    case VMAP_VOXEL_I16: fuse_dispatch<VMAP_VOXEL_I16>(m, color, f, grid, s); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_reset(const DevMap& m, size_t poolBytes, const Launcher& l, cudaStream_t s)
+{
+    reset_hash_kernel<<<l.numSMs * 4, 256, 0, s>>>(m);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(m.ctr, 0, C_COUNT * sizeof(unsigned), s)) != cudaSuccess) return e;
+    return cudaMemsetAsync(m.pool, 0, poolBytes, s);
+}
+
+}  // namespace vmapb

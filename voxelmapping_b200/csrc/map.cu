@@ -1,0 +1,662 @@
+// C ABI of libvmap_b200 (include/vmap_c.h): map lifetime, argument checking,
+// pose handling (FP64 on the host) and kernel sequencing. No call here
+// synchronises the device except the documented synchronous entry points.
+//
+// Reference: src/vmapping.cpp (VoxelizationImpl :10-148), src/map_struct.cu
+// (create / reset / release :29-79).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "vmap_launch.h"
+
+using namespace vmapb;
+
+struct vmap_map {
+    vmap_config cfg;
+    DevMap dm;
+    Launcher launcher;
+    int device;
+    size_t poolBytes;
+    size_t deviceBytes;
+    unsigned* hCtr;           // pinned readback of the counters
+    unsigned* zmin;           // z-range tiles
+    unsigned* zmax;
+    int tilesX, tilesY;
+    void* dDepth;             // staging for host-buffer calls
+    uint8_t* dRgb;
+    float4* dVmap;
+    float4* dNmap;
+    float* dVerts;            // mesh buffers of vmap_polygonize_host
+    float* dNorms;
+    float* hVerts;
+    float* hNorms;
+    unsigned meshCap;
+    unsigned* dNtri;
+    // stage timing: event pairs on the caller's stream
+    unsigned tCap, tUsed;
+    cudaEvent_t* tEv;
+    int* tStage;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+vmap_status cuda_fail(cudaError_t e, const char* what)
+{
+    g_last_error = std::string(what) + ": " + cudaGetErrorString(e);
+    return e == cudaErrorMemoryAllocation ? VMAP_ERR_OUT_OF_MEMORY : VMAP_ERR_CUDA;
+}
+
+#define VMAP_CK(expr)                                          \
+    do {                                                       \
+        cudaError_t e_ = (expr);                               \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #expr);    \
+    } while (0)
+
+inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
+
+void to_xf(const double p[16], Xf& t)
+{
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) t.m[r][c] = (float)p[4 * r + c];
+}
+
+bool pose_ok(const double p[16])
+{
+    if (!p) return false;
+    for (int i = 0; i < 12; ++i)
+        if (!std::isfinite(p[i])) return false;
+    return true;
+}
+
+void make_frame(const vmap_map* m, const double pose[16], FrameParams& f)
+{
+    f.W = m->cfg.width;
+    f.H = m->cfg.height;
+    f.fx = m->cfg.fx;
+    f.fy = m->cfg.fy;
+    f.cx = m->cfg.cx;
+    f.cy = m->cfg.cy;
+    f.ifx = (float)(1.0 / (double)m->cfg.fx);
+    f.ify = (float)(1.0 / (double)m->cfg.fy);
+    double inv[16];
+    vmap_pose_inverse(pose, inv);
+    to_xf(pose, f.T);
+    to_xf(inv, f.Ti);
+    f.depth = nullptr;
+    f.dpitch = 0;
+    f.dtype = 0;
+    f.dscale = 1.f;
+    f.rgb = nullptr;
+    f.rgbPitch = 0;
+}
+
+template <typename T>
+cudaError_t dalloc(vmap_map* m, T** p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc((void**)p, bytes ? bytes : 16);
+    if (e == cudaSuccess) m->deviceBytes += bytes;
+    return e;
+}
+
+void timing_free(vmap_map* m)
+{
+    for (unsigned i = 0; i < 2 * m->tCap; ++i) cudaEventDestroy(m->tEv[i]);
+    delete[] m->tEv;
+    delete[] m->tStage;
+    m->tEv = nullptr;
+    m->tStage = nullptr;
+    m->tCap = m->tUsed = 0;
+}
+
+// Runs one kernel launcher, bracketed by timing events when timing is on.
+template <typename F>
+cudaError_t staged(vmap_map* m, int stage, cudaStream_t s, F&& launch)
+{
+    const bool rec = m->tUsed < m->tCap;
+    if (rec) cudaEventRecord(m->tEv[2 * m->tUsed], s);
+    cudaError_t e = launch();
+    if (rec && e == cudaSuccess) {
+        cudaEventRecord(m->tEv[2 * m->tUsed + 1], s);
+        m->tStage[m->tUsed++] = stage;
+    }
+    return e;
+}
+
+void free_all(vmap_map* m)
+{
+    timing_free(m);
+    cudaFree(m->dm.keys);
+    cudaFree(m->dm.vals);
+    cudaFree(m->dm.blockKeys);
+    cudaFree(m->dm.pool);
+    cudaFree(m->dm.ctr);
+    cudaFree(m->dm.visList);
+    cudaFree(m->zmin);
+    cudaFree(m->zmax);
+    cudaFree(m->dDepth);
+    cudaFree(m->dRgb);
+    cudaFree(m->dVmap);
+    cudaFree(m->dNmap);
+    cudaFree(m->dVerts);
+    cudaFree(m->dNorms);
+    cudaFree(m->dNtri);
+    if (m->hCtr) cudaFreeHost(m->hCtr);
+    if (m->hVerts) cudaFreeHost(m->hVerts);
+    if (m->hNorms) cudaFreeHost(m->hNorms);
+}
+
+}  // namespace
+
+extern "C" {
+
+int vmap_abi_version(void) { return VMAP_ABI_VERSION; }
+
+const char* vmap_last_error(void) { return g_last_error.c_str(); }
+
+const char* vmap_status_string(vmap_status s)
+{
+    switch (s) {
+    case VMAP_OK: return "ok";
+    case VMAP_ERR_INVALID_ARG: return "invalid argument";
+    case VMAP_ERR_CUDA: return "CUDA error";
+    case VMAP_ERR_OUT_OF_MEMORY: return "out of memory";
+    case VMAP_ERR_POOL_FULL: return "voxel-block pool full";
+    case VMAP_ERR_HASH_FULL: return "hash table full";
+    case VMAP_ERR_RANGE: return "block coordinate out of range";
+    case VMAP_ERR_BUFFER_FULL: return "mesh buffer full";
+    case VMAP_ERR_NO_DEVICE: return "no sm_100 CUDA device";
+    }
+    return "unknown status";
+}
+
+// hash (map_struct.h:104-109), host copy for tests
+int vmap_block_hash(int x, int y, int z, int nb)
+{
+    int r = (int)(((unsigned)x * 73856093u) ^ ((unsigned)y * 19349669u) ^ ((unsigned)z * 83492791u));
+    r %= nb;
+    return r < 0 ? r + nb : r;
+}
+
+// Affine inverse of a row-major camera-to-world pose in double:
+// inv(A) = adj(A) / det(A), t' = -inv(A) t (the reference inverts the 4x4 in
+// float with Eigen, depth_fusion.cu:251, ray_tracing.cu:414).
+void vmap_pose_inverse(const double p[16], double o[16])
+{
+    const double a = p[0], b = p[1], c = p[2], d = p[4], e = p[5], f = p[6], g = p[8], h = p[9], i = p[10];
+    const double A = e * i - f * h, B = f * g - d * i, C = d * h - e * g;
+    const double det = a * A + b * B + c * C;
+    const double r = 1.0 / det;
+    o[0] = A * r;
+    o[1] = (c * h - b * i) * r;
+    o[2] = (b * f - c * e) * r;
+    o[4] = B * r;
+    o[5] = (a * i - c * g) * r;
+    o[6] = (c * d - a * f) * r;
+    o[8] = C * r;
+    o[9] = (b * g - a * h) * r;
+    o[10] = (a * e - b * d) * r;
+    for (int k = 0; k < 3; ++k) o[4 * k + 3] = -(o[4 * k] * p[3] + o[4 * k + 1] * p[7] + o[4 * k + 2] * p[11]);
+    o[12] = o[13] = o[14] = 0.0;
+    o[15] = 1.0;
+}
+
+size_t vmap_block_bytes(int fmt, int color)
+{
+    switch (fmt) {
+    case VMAP_VOXEL_REF: return Layout<VMAP_VOXEL_REF>::bytes(color != 0);
+    case VMAP_VOXEL_F32: return Layout<VMAP_VOXEL_F32>::bytes(color != 0);
+    case VMAP_VOXEL_F16: return Layout<VMAP_VOXEL_F16>::bytes(color != 0);
+    case VMAP_VOXEL_I16: return Layout<VMAP_VOXEL_I16>::bytes(color != 0);
+    }
+    return 0;
+}
+
+vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
+{
+    if (!cfg_in || !out) return VMAP_ERR_INVALID_ARG;
+    *out = nullptr;
+    vmap_config cfg = *cfg_in;
+    if (cfg.width <= 0 || cfg.height <= 0 || !(cfg.fx > 0) || !(cfg.fy > 0) || !std::isfinite(cfg.cx) ||
+        !std::isfinite(cfg.cy) || cfg.num_blocks <= 0 || !(cfg.voxel_size > 0) || cfg.num_entries < 0 ||
+        cfg.num_buckets < 0 || cfg.truncation < 0 || cfg.max_weight < 0 || cfg.raycast_mode < 0 ||
+        cfg.raycast_mode > 1)
+        return VMAP_ERR_INVALID_ARG;
+    const size_t blockBytes = vmap_block_bytes(cfg.voxel_format, cfg.with_color);
+    if (blockBytes == 0) return VMAP_ERR_INVALID_ARG;
+    if (cfg.num_buckets == 0) cfg.num_buckets = (int)(cfg.num_blocks * 0.9);  // vmapping.cpp:59
+    if (cfg.num_buckets < 1) cfg.num_buckets = 1;
+    if ((long long)cfg.num_buckets * kSlots < (long long)cfg.num_entries)
+        cfg.num_buckets = (int)(((long long)cfg.num_entries + kSlots - 1) / kSlots);
+    if (cfg.truncation == 0) cfg.truncation = cfg.voxel_size * 4;  // vmapping.cpp:59
+    if (cfg.max_weight == 0) cfg.max_weight = 255;                 // depth_fusion.cu:193
+    if (cfg.voxel_format == VMAP_VOXEL_REF && cfg.max_weight > 255) return VMAP_ERR_INVALID_ARG;
+    if (cfg.max_weight > 65535) return VMAP_ERR_INVALID_ARG;
+
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return (cuda_fail(e, "cudaGetDevice"), VMAP_ERR_NO_DEVICE);
+    cudaDeviceProp prop;
+    if ((e = cudaGetDeviceProperties(&prop, dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
+    if (prop.major != 10) {
+        g_last_error = "libvmap_b200 is built for sm_100a; device is sm_" + std::to_string(prop.major * 10 + prop.minor);
+        return VMAP_ERR_NO_DEVICE;
+    }
+
+    vmap_map* m = new (std::nothrow) vmap_map();
+    if (!m) return VMAP_ERR_OUT_OF_MEMORY;
+    std::memset(m, 0, sizeof(*m));
+    m->cfg = cfg;
+    m->device = dev;
+    m->launcher.numSMs = prop.multiProcessorCount;
+    m->tilesX = (cfg.width + kZTile - 1) / kZTile;
+    m->tilesY = (cfg.height + kZTile - 1) / kZTile;
+    const size_t nslots = (size_t)cfg.num_buckets * kSlots, cap = (size_t)cfg.num_blocks;
+    const size_t npix = (size_t)cfg.width * cfg.height, ntiles = (size_t)m->tilesX * m->tilesY;
+    m->poolBytes = cap * blockBytes;
+#define VMAP_ALLOC(ptr, bytes)                                        \
+    do {                                                              \
+        cudaError_t e2 = dalloc(m, &(ptr), (bytes));                  \
+        if (e2 != cudaSuccess) {                                      \
+            vmap_status st = cuda_fail(e2, "cudaMalloc " #ptr);        \
+            free_all(m);                                              \
+            delete m;                                                 \
+            return st;                                                \
+        }                                                             \
+    } while (0)
+    VMAP_ALLOC(m->dm.keys, nslots * sizeof(unsigned long long));
+    VMAP_ALLOC(m->dm.vals, nslots * sizeof(int));
+    VMAP_ALLOC(m->dm.blockKeys, cap * sizeof(unsigned long long));
+    VMAP_ALLOC(m->dm.pool, m->poolBytes);
+    VMAP_ALLOC(m->dm.ctr, C_COUNT * sizeof(unsigned));
+    VMAP_ALLOC(m->dm.visList, cap * sizeof(int));
+    VMAP_ALLOC(m->zmin, ntiles * sizeof(unsigned));
+    VMAP_ALLOC(m->zmax, ntiles * sizeof(unsigned));
+    VMAP_ALLOC(m->dDepth, npix * sizeof(float));
+    VMAP_ALLOC(m->dRgb, npix * 3);
+    VMAP_ALLOC(m->dVmap, npix * sizeof(float4));
+    VMAP_ALLOC(m->dNmap, npix * sizeof(float4));
+    VMAP_ALLOC(m->dNtri, sizeof(unsigned));
+#undef VMAP_ALLOC
+    if ((e = cudaHostAlloc((void**)&m->hCtr, C_COUNT * sizeof(unsigned), cudaHostAllocDefault)) != cudaSuccess) {
+        vmap_status st = cuda_fail(e, "cudaHostAlloc");
+        free_all(m);
+        delete m;
+        return st;
+    }
+    m->dm.nBucket = cfg.num_buckets;
+    m->dm.capacity = cfg.num_blocks;
+    m->dm.blockBytes = (int)blockBytes;
+    m->dm.vs = cfg.voxel_size;
+    m->dm.mu = cfg.truncation;
+    m->dm.wmax = (float)cfg.max_weight;
+    vmap_status st = vmap_reset(m, nullptr);
+    if (st == VMAP_OK && (e = cudaStreamSynchronize(nullptr)) != cudaSuccess) st = cuda_fail(e, "create sync");
+    if (st != VMAP_OK) {
+        free_all(m);
+        delete m;
+        return st;
+    }
+    *out = m;
+    return VMAP_OK;
+}
+
+vmap_status vmap_destroy(vmap_map* m)
+{
+    if (!m) return VMAP_ERR_INVALID_ARG;
+    cudaDeviceSynchronize();
+    free_all(m);
+    delete m;
+    return VMAP_OK;
+}
+
+vmap_status vmap_get_config(const vmap_map* m, vmap_config* out)
+{
+    if (!m || !out) return VMAP_ERR_INVALID_ARG;
+    *out = m->cfg;
+    return VMAP_OK;
+}
+
+vmap_status vmap_reset(vmap_map* m, void* stream)
+{
+    if (!m) return VMAP_ERR_INVALID_ARG;
+    VMAP_CK(launch_reset(m->dm, m->poolBytes, m->launcher, as_stream(stream)));
+    return VMAP_OK;
+}
+
+static vmap_status fuse_impl(vmap_map* m, const void* depth, int dtype, size_t dpitch, float dscale,
+                             const uint8_t* rgb, size_t rgbPitch, const double pose[16], cudaStream_t s)
+{
+    if (!m || !depth || !pose_ok(pose)) return VMAP_ERR_INVALID_ARG;
+    if (dtype != VMAP_DEPTH_F32 && dtype != VMAP_DEPTH_U16) return VMAP_ERR_INVALID_ARG;
+    const size_t elem = dtype == VMAP_DEPTH_F32 ? 4 : 2;
+    if (dpitch == 0) dpitch = elem * m->cfg.width;
+    if (dpitch < elem * m->cfg.width || dpitch % elem) return VMAP_ERR_INVALID_ARG;
+    if (dtype == VMAP_DEPTH_U16 && !(dscale > 0)) return VMAP_ERR_INVALID_ARG;
+    if (rgb) {
+        if (!m->cfg.with_color) return VMAP_ERR_INVALID_ARG;
+        if (rgbPitch == 0) rgbPitch = 3 * (size_t)m->cfg.width;
+        if (rgbPitch < 3 * (size_t)m->cfg.width) return VMAP_ERR_INVALID_ARG;
+    }
+    FrameParams f;
+    make_frame(m, pose, f);
+    f.depth = depth;
+    f.dpitch = dpitch;
+    f.dtype = dtype;
+    f.dscale = dscale;
+    f.rgb = rgb;
+    f.rgbPitch = rgbPitch;
+    VMAP_CK(staged(m, VMAP_STAGE_ALLOC, s, [&] { return launch_alloc(m->dm, f, m->launcher, s); }));
+    VMAP_CK(staged(m, VMAP_STAGE_VISIBILITY, s, [&] { return launch_visibility(m->dm, f, m->launcher, s); }));
+    VMAP_CK(staged(m, VMAP_STAGE_FUSE, s,
+                   [&] { return launch_fuse(m->dm, m->cfg.voxel_format, rgb != nullptr, f, m->launcher, s); }));
+    return VMAP_OK;
+}
+
+vmap_status vmap_fuse_depth(vmap_map* m, const void* depth_dev, int depth_type, size_t depth_pitch,
+                            float depth_scale, const double pose[16], void* stream)
+{
+    return fuse_impl(m, depth_dev, depth_type, depth_pitch, depth_scale, nullptr, 0, pose, as_stream(stream));
+}
+
+vmap_status vmap_fuse_depth_rgb(vmap_map* m, const void* depth_dev, int depth_type, size_t depth_pitch,
+                                float depth_scale, const uint8_t* rgb_dev, size_t rgb_pitch, const double pose[16],
+                                void* stream)
+{
+    if (!rgb_dev) return VMAP_ERR_INVALID_ARG;
+    return fuse_impl(m, depth_dev, depth_type, depth_pitch, depth_scale, rgb_dev, rgb_pitch, pose,
+                     as_stream(stream));
+}
+
+vmap_status vmap_fuse_host(vmap_map* m, const void* depth_host, int depth_type, float depth_scale,
+                           const uint8_t* rgb_host, const double pose[16], void* stream)
+{
+    if (!m || !depth_host) return VMAP_ERR_INVALID_ARG;
+    if (depth_type != VMAP_DEPTH_F32 && depth_type != VMAP_DEPTH_U16) return VMAP_ERR_INVALID_ARG;
+    if (rgb_host && !m->cfg.with_color) return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    const size_t npix = (size_t)m->cfg.width * m->cfg.height;
+    const size_t elem = depth_type == VMAP_DEPTH_F32 ? 4 : 2;
+    VMAP_CK(cudaMemcpyAsync(m->dDepth, depth_host, npix * elem, cudaMemcpyHostToDevice, s));
+    if (rgb_host) VMAP_CK(cudaMemcpyAsync(m->dRgb, rgb_host, npix * 3, cudaMemcpyHostToDevice, s));
+    return fuse_impl(m, m->dDepth, depth_type, elem * m->cfg.width, depth_scale, rgb_host ? m->dRgb : nullptr,
+                     3 * (size_t)m->cfg.width, pose, s);
+}
+
+vmap_status vmap_check_visible_blocks(vmap_map* m, const double pose[16], void* stream)
+{
+    if (!m || !pose_ok(pose)) return VMAP_ERR_INVALID_ARG;
+    FrameParams f;
+    make_frame(m, pose, f);
+    cudaStream_t s = as_stream(stream);
+    VMAP_CK(staged(m, VMAP_STAGE_VISIBILITY, s, [&] { return launch_visibility(m->dm, f, m->launcher, s); }));
+    return VMAP_OK;
+}
+
+vmap_status vmap_render_scene(vmap_map* m, const double pose[16], float* vmap_dev, size_t vmap_pitch,
+                              float* nmap_dev, size_t nmap_pitch, void* stream)
+{
+    if (!m || !vmap_dev || !pose_ok(pose)) return VMAP_ERR_INVALID_ARG;
+    const size_t row = sizeof(float4) * (size_t)m->cfg.width;
+    if (vmap_pitch == 0) vmap_pitch = row;
+    if (nmap_pitch == 0) nmap_pitch = row;
+    if (vmap_pitch < row || vmap_pitch % 16 || (nmap_dev && (nmap_pitch < row || nmap_pitch % 16)) ||
+        ((uintptr_t)vmap_dev & 15) || ((uintptr_t)nmap_dev & 15))
+        return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    RenderParams r;
+    r.W = m->cfg.width;
+    r.H = m->cfg.height;
+    r.fx = m->cfg.fx;
+    r.fy = m->cfg.fy;
+    r.cx = m->cfg.cx;
+    r.cy = m->cfg.cy;
+    r.ifx = (float)(1.0 / (double)m->cfg.fx);
+    r.ify = (float)(1.0 / (double)m->cfg.fy);
+    r.vsinv = (float)(1.0 / (double)m->cfg.voxel_size);
+    r.rts = m->cfg.truncation / m->cfg.voxel_size;
+    double inv[16];
+    vmap_pose_inverse(pose, inv);
+    to_xf(pose, r.T);
+    to_xf(inv, r.Ti);
+    r.mode = m->cfg.raycast_mode;
+    r.tilesX = m->tilesX;
+    r.tilesY = m->tilesY;
+    r.zmin = m->zmin;
+    r.zmax = m->zmax;
+    if (r.mode == 0)
+        VMAP_CK(staged(m, VMAP_STAGE_ZRANGE, s, [&] { return launch_zrange(m->dm, r, m->launcher, s); }));
+    VMAP_CK(staged(m, VMAP_STAGE_RAYCAST, s, [&] {
+        return launch_raycast(m->dm, m->cfg.voxel_format, r, reinterpret_cast<float4*>(vmap_dev), vmap_pitch,
+                              m->launcher, s);
+    }));
+    if (nmap_dev)
+        VMAP_CK(staged(m, VMAP_STAGE_NORMALS, s, [&] {
+            return launch_normals(reinterpret_cast<const float4*>(vmap_dev), vmap_pitch,
+                                  reinterpret_cast<float4*>(nmap_dev), nmap_pitch, r.W, r.H, s);
+        }));
+    return VMAP_OK;
+}
+
+vmap_status vmap_render_scene_host(vmap_map* m, const double pose[16], float* vmap_host, float* nmap_host,
+                                   void* stream)
+{
+    if (!m || !vmap_host) return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    vmap_status st = vmap_render_scene(m, pose, (float*)m->dVmap, 0, nmap_host ? (float*)m->dNmap : nullptr, 0, stream);
+    if (st != VMAP_OK) return st;
+    const size_t bytes = (size_t)m->cfg.width * m->cfg.height * sizeof(float4);
+    VMAP_CK(cudaMemcpyAsync(vmap_host, m->dVmap, bytes, cudaMemcpyDeviceToHost, s));
+    if (nmap_host) VMAP_CK(cudaMemcpyAsync(nmap_host, m->dNmap, bytes, cudaMemcpyDeviceToHost, s));
+    return VMAP_OK;
+}
+
+vmap_status vmap_compute_normal(const float* vmap_dev, size_t vmap_pitch, float* nmap_dev, size_t nmap_pitch,
+                                int width, int height, void* stream)
+{
+    if (!vmap_dev || !nmap_dev || width <= 0 || height <= 0) return VMAP_ERR_INVALID_ARG;
+    const size_t row = sizeof(float4) * (size_t)width;
+    if (vmap_pitch == 0) vmap_pitch = row;
+    if (nmap_pitch == 0) nmap_pitch = row;
+    if (vmap_pitch < row || nmap_pitch < row || vmap_pitch % 16 || nmap_pitch % 16) return VMAP_ERR_INVALID_ARG;
+    VMAP_CK(launch_normals(reinterpret_cast<const float4*>(vmap_dev), vmap_pitch, reinterpret_cast<float4*>(nmap_dev),
+                           nmap_pitch, width, height, as_stream(stream)));
+    return VMAP_OK;
+}
+
+vmap_status vmap_render_phong(const float* vmap_dev, size_t vmap_pitch, const float* nmap_dev, size_t nmap_pitch,
+                              uint8_t* rgba_dev, size_t rgba_pitch, int width, int height, void* stream)
+{
+    if (!vmap_dev || !nmap_dev || !rgba_dev || width <= 0 || height <= 0) return VMAP_ERR_INVALID_ARG;
+    const size_t row = sizeof(float4) * (size_t)width;
+    if (vmap_pitch == 0) vmap_pitch = row;
+    if (nmap_pitch == 0) nmap_pitch = row;
+    if (rgba_pitch == 0) rgba_pitch = 4 * (size_t)width;
+    if (vmap_pitch < row || nmap_pitch < row || rgba_pitch < 4 * (size_t)width || rgba_pitch % 4)
+        return VMAP_ERR_INVALID_ARG;
+    VMAP_CK(launch_phong(reinterpret_cast<const float4*>(vmap_dev), vmap_pitch,
+                         reinterpret_cast<const float4*>(nmap_dev), nmap_pitch, reinterpret_cast<uchar4*>(rgba_dev),
+                         rgba_pitch, width, height, as_stream(stream)));
+    return VMAP_OK;
+}
+
+vmap_status vmap_polygonize(vmap_map* m, float* verts_dev, float* norms_dev, uint32_t max_tris, uint32_t* n_tris_dev,
+                            void* stream)
+{
+    if (!m || (norms_dev && !verts_dev)) return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    VMAP_CK(staged(m, VMAP_STAGE_MESH, s, [&] {
+        return launch_mesh(m->dm, m->cfg.voxel_format, verts_dev, norms_dev, verts_dev ? max_tris : 0u, n_tris_dev,
+                           m->launcher, s);
+    }));
+    return VMAP_OK;
+}
+
+vmap_status vmap_polygonize_host(vmap_map* m, const float** verts, const float** norms, uint32_t* n_tris, void* stream)
+{
+    if (!m || !verts || !norms || !n_tris) return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    unsigned count = 0;
+    VMAP_CK(launch_mesh(m->dm, m->cfg.voxel_format, nullptr, nullptr, 0u, m->dNtri, m->launcher, s));
+    VMAP_CK(cudaMemcpyAsync(&count, m->dNtri, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    VMAP_CK(cudaStreamSynchronize(s));
+    if (count > m->meshCap) {
+        cudaFree(m->dVerts);
+        cudaFree(m->dNorms);
+        if (m->hVerts) cudaFreeHost(m->hVerts);
+        if (m->hNorms) cudaFreeHost(m->hNorms);
+        m->dVerts = m->dNorms = m->hVerts = m->hNorms = nullptr;
+        m->meshCap = 0;
+        const unsigned cap = count + count / 8 + 1024;
+        const size_t bytes = (size_t)cap * 9 * sizeof(float);
+        VMAP_CK(cudaMalloc((void**)&m->dVerts, bytes));
+        VMAP_CK(cudaMalloc((void**)&m->dNorms, bytes));
+        VMAP_CK(cudaHostAlloc((void**)&m->hVerts, bytes, cudaHostAllocDefault));
+        VMAP_CK(cudaHostAlloc((void**)&m->hNorms, bytes, cudaHostAllocDefault));
+        m->meshCap = cap;
+    }
+    if (count > 0) {
+        VMAP_CK(launch_mesh(m->dm, m->cfg.voxel_format, m->dVerts, m->dNorms, m->meshCap, m->dNtri, m->launcher, s));
+        VMAP_CK(cudaMemcpyAsync(&count, m->dNtri, sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        VMAP_CK(cudaStreamSynchronize(s));
+        if (count > m->meshCap) count = m->meshCap;
+        const size_t bytes = (size_t)count * 9 * sizeof(float);
+        VMAP_CK(cudaMemcpyAsync(m->hVerts, m->dVerts, bytes, cudaMemcpyDeviceToHost, s));
+        VMAP_CK(cudaMemcpyAsync(m->hNorms, m->dNorms, bytes, cudaMemcpyDeviceToHost, s));
+        VMAP_CK(cudaStreamSynchronize(s));
+    }
+    *verts = m->hVerts;
+    *norms = m->hNorms;
+    *n_tris = count;
+    return VMAP_OK;
+}
+
+vmap_status vmap_surface_points(const float* verts_dev, uint32_t n_tris, float* points_dev, void* stream)
+{
+    if ((!verts_dev || !points_dev) && n_tris) return VMAP_ERR_INVALID_ARG;
+    VMAP_CK(launch_surface_points(verts_dev, n_tris, points_dev, as_stream(stream)));
+    return VMAP_OK;
+}
+
+vmap_status vmap_get_stats(vmap_map* m, void* stream, vmap_stats* out)
+{
+    if (!m || !out) return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = as_stream(stream);
+    VMAP_CK(cudaMemcpyAsync(m->hCtr, m->dm.ctr, C_COUNT * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    VMAP_CK(cudaStreamSynchronize(s));
+    const unsigned alloc = m->hCtr[C_ALLOC];
+    out->allocated_blocks = alloc < (unsigned)m->cfg.num_blocks ? alloc : (unsigned)m->cfg.num_blocks;
+    out->capacity_blocks = (unsigned)m->cfg.num_blocks;
+    out->visible_blocks = m->hCtr[C_VISIBLE];
+    out->error_flags = m->hCtr[C_ERR];
+    out->failed_allocs = m->hCtr[C_FAILED];
+    out->last_triangles = m->hCtr[C_TRI];
+    out->pool_bytes = m->poolBytes;
+    out->device_bytes = m->deviceBytes;
+    return VMAP_OK;
+}
+
+vmap_status vmap_clear_errors(vmap_map* m, void* stream)
+{
+    if (!m) return VMAP_ERR_INVALID_ARG;
+    VMAP_CK(cudaMemsetAsync(m->dm.ctr + C_ERR, 0, sizeof(unsigned), as_stream(stream)));
+    VMAP_CK(cudaMemsetAsync(m->dm.ctr + C_FAILED, 0, sizeof(unsigned), as_stream(stream)));
+    return VMAP_OK;
+}
+
+vmap_status vmap_copy_counters(vmap_map* m, uint32_t* dst, void* stream)
+{
+    if (!m || !dst) return VMAP_ERR_INVALID_ARG;
+    VMAP_CK(cudaMemcpyAsync(dst, m->dm.ctr, C_COUNT * sizeof(unsigned), cudaMemcpyDefault, as_stream(stream)));
+    return VMAP_OK;
+}
+
+vmap_status vmap_timing_enable(vmap_map* m, uint32_t max_records)
+{
+    if (!m) return VMAP_ERR_INVALID_ARG;
+    timing_free(m);
+    if (max_records == 0) return VMAP_OK;
+    m->tEv = new (std::nothrow) cudaEvent_t[2 * (size_t)max_records];
+    m->tStage = new (std::nothrow) int[max_records];
+    if (!m->tEv || !m->tStage) {
+        timing_free(m);
+        return VMAP_ERR_OUT_OF_MEMORY;
+    }
+    for (uint32_t i = 0; i < 2 * max_records; ++i) {
+        cudaError_t e = cudaEventCreate(&m->tEv[i]);
+        if (e != cudaSuccess) {
+            m->tCap = i / 2;
+            timing_free(m);
+            return cuda_fail(e, "cudaEventCreate");
+        }
+        m->tCap = (i + 1) / 2;
+    }
+    m->tCap = max_records;
+    m->tUsed = 0;
+    return VMAP_OK;
+}
+
+vmap_status vmap_timing_read(vmap_map* m, double ms[VMAP_NUM_STAGES], uint32_t launches[VMAP_NUM_STAGES])
+{
+    if (!m || !ms || !launches) return VMAP_ERR_INVALID_ARG;
+    for (int i = 0; i < VMAP_NUM_STAGES; ++i) {
+        ms[i] = 0.0;
+        launches[i] = 0;
+    }
+    for (unsigned i = 0; i < m->tUsed; ++i) {
+        VMAP_CK(cudaEventSynchronize(m->tEv[2 * i + 1]));
+        float t = 0.f;
+        VMAP_CK(cudaEventElapsedTime(&t, m->tEv[2 * i], m->tEv[2 * i + 1]));
+        ms[m->tStage[i]] += t;
+        launches[m->tStage[i]]++;
+    }
+    m->tUsed = 0;
+    return VMAP_OK;
+}
+
+vmap_status vmap_export_blocks(vmap_map* m, int32_t* coords, float* tsdf, float* weight, uint8_t* rgb,
+                               uint32_t max_blocks, uint32_t* n_blocks, void* stream)
+{
+    if (!m || !n_blocks) return VMAP_ERR_INVALID_ARG;
+    if (rgb && !m->cfg.with_color) return VMAP_ERR_INVALID_ARG;
+    vmap_stats st;
+    vmap_status r = vmap_get_stats(m, stream, &st);
+    if (r != VMAP_OK) return r;
+    *n_blocks = st.allocated_blocks;
+    const uint32_t n = st.allocated_blocks < max_blocks ? st.allocated_blocks : max_blocks;
+    if (n == 0 || (!coords && !tsdf && !weight && !rgb)) return VMAP_OK;
+    cudaStream_t s = as_stream(stream);
+    const int chunk = 8192;
+    int* dc = nullptr;
+    float *dt = nullptr, *dw = nullptr;
+    uint8_t* drgb = nullptr;
+    cudaError_t e = cudaMalloc((void**)&dc, (size_t)chunk * 3 * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&dt, (size_t)chunk * 512 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&dw, (size_t)chunk * 512 * sizeof(float));
+    if (e == cudaSuccess && rgb) e = cudaMalloc((void**)&drgb, (size_t)chunk * 512 * 3);
+    for (uint32_t first = 0; e == cudaSuccess && first < n; first += chunk) {
+        const int cnt = (int)((n - first) < (uint32_t)chunk ? (n - first) : (uint32_t)chunk);
+        e = launch_export(m->dm, m->cfg.voxel_format, rgb != nullptr, (int)first, cnt, dc, dt, dw, drgb, s);
+        if (e == cudaSuccess && coords)
+            e = cudaMemcpyAsync(coords + 3 * (size_t)first, dc, (size_t)cnt * 3 * sizeof(int), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && tsdf)
+            e = cudaMemcpyAsync(tsdf + 512 * (size_t)first, dt, (size_t)cnt * 512 * sizeof(float), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && weight)
+            e = cudaMemcpyAsync(weight + 512 * (size_t)first, dw, (size_t)cnt * 512 * sizeof(float), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess && rgb)
+            e = cudaMemcpyAsync(rgb + 3 * 512 * (size_t)first, drgb, (size_t)cnt * 512 * 3, cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    }
+    cudaFree(dc);
+    cudaFree(dt);
+    cudaFree(dw);
+    cudaFree(drgb);
+    if (e != cudaSuccess) return cuda_fail(e, "vmap_export_blocks");
+    return VMAP_OK;
+}
+
+}  // extern "C"

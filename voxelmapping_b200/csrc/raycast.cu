@@ -1,0 +1,351 @@
+// Raycast path: per-tile depth bounds, ray marching with trilinear
+// interpolation, normal map and Phong preview.
+//
+// Reference: src/ray_tracing.cu (RenderingBlockDelegate :13-137,
+// FillRenderingBlockFunctor :139-169, MapRenderingDelegate :255-401) and
+// src/image_proc.cu (renderSceneKernel :8-61, computeNormalKernel :74-93).
+//
+// The reference marches every ray from z = 0.1 m to 5 m, one voxel per step
+// through unallocated space, with a full hash-chain walk per sample; it
+// computes per-tile z ranges but never reads them (ray_tracing.cu:335-341).
+// This implementation keeps the reference's sample lattice (start point,
+// direction, 1-voxel steps in empty space, SDF-proportional steps near
+// surfaces, two refinement steps) and skips work that cannot change the
+// result:
+//   * tiles of 8x8 pixels start at the nearest allocated block that can
+//     cover them and stop after the farthest one (bounds computed over all
+//     allocated blocks, conservatively, so no block a ray can enter is
+//     missed);
+//   * inside an unallocated block, where the reference reads "invalid, 1.0"
+//     and steps 1 voxel at a time, the steps up to the block's exit are taken
+//     as one integer jump;
+//   * block lookups are cached per thread.
+#include "vmap_launch.h"
+
+namespace vmapb {
+
+// ------------------------------------------------------------------ z-range
+// Per allocated block: project the 8 corners, take the pixel bounding box
+// (+1 px) and depth range (+-1 voxel), and fold them into the tile maps with
+// integer atomics (depths are positive, so float order == bit order). A block
+// with a corner at or behind z = 0.05 m covers every tile from depth 0.
+__global__ void __launch_bounds__(256) zrange_kernel(DevMap m, RenderParams r)
+{
+    const int n = allocated_blocks(m);
+    const float scale = m.vs * 8.f;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int3 b = unpack_key(m.blockKeys[i]);
+        float zlo = 1e30f, zhi = -1e30f, umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+        bool near = false;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const float3 p = xf_apply(r.Ti, (float)(b.x + (c & 1)) * scale, (float)(b.y + ((c >> 1) & 1)) * scale,
+                                      (float)(b.z + ((c >> 2) & 1)) * scale);
+            zlo = fminf(zlo, p.z);
+            zhi = fmaxf(zhi, p.z);
+            if (p.z <= 0.05f) {
+                near = true;
+                continue;
+            }
+            const float u = r.fx * p.x / p.z + r.cx, v = r.fy * p.y / p.z + r.cy;
+            umin = fminf(umin, u);
+            umax = fmaxf(umax, u);
+            vmin = fminf(vmin, v);
+            vmax = fmaxf(vmax, v);
+        }
+        if (zhi < kMinDepth - m.vs || zlo > kMaxDepth + m.vs) continue;
+        int tx0 = 0, tx1 = r.tilesX - 1, ty0 = 0, ty1 = r.tilesY - 1;
+        if (!near) {
+            if (umax < -1.f || vmax < -1.f || umin > (float)r.W || vmin > (float)r.H) continue;
+            tx0 = max(0, (int)floorf(umin - 1.f) >> 3);
+            tx1 = min(r.tilesX - 1, (int)floorf(umax + 1.f) >> 3);
+            ty0 = max(0, (int)floorf(vmin - 1.f) >> 3);
+            ty1 = min(r.tilesY - 1, (int)floorf(vmax + 1.f) >> 3);
+        }
+        const unsigned lo = __float_as_uint(near ? 0.f : fmaxf(zlo - m.vs, 0.f));
+        const unsigned hi = __float_as_uint(zhi + m.vs);
+        for (int ty = ty0; ty <= ty1; ++ty)
+            for (int tx = tx0; tx <= tx1; ++tx) {
+                const int t = ty * r.tilesX + tx;
+                atomicMin(r.zmin + t, lo);
+                atomicMax(r.zmax + t, hi);
+            }
+    }
+}
+
+// ------------------------------------------------------------------ raycast
+template <int FMT>
+struct RayCtx {
+    const DevMap& m;
+    int cbx, cby, cbz, cblk;  // block of the current sample
+    int obx, oby, obz, oblk;  // last other block (trilinear corners)
+
+    __device__ __forceinline__ RayCtx(const DevMap& mm) : m(mm), cbx(INT_MIN), cby(0), cbz(0), cblk(-1),
+        obx(INT_MIN), oby(0), obz(0), oblk(-1) {}
+
+    __device__ __forceinline__ int block_of(int bx, int by, int bz)
+    {
+        if (bx == cbx && by == cby && bz == cbz) return cblk;
+        if (bx == obx && by == oby && bz == obz) return oblk;
+        obx = bx;
+        oby = by;
+        obz = bz;
+        oblk = hash_find(m, bx, by, bz);
+        return oblk;
+    }
+
+    // read_sdf (ray_tracing.cu:272-286): voxel at integer coordinates;
+    // unallocated or zero weight -> invalid, 1.0
+    __device__ __forceinline__ float voxel(int slot, int vx, int vy, int vz, bool& valid) const
+    {
+        if (slot >= 0) {
+            const int li = local_idx(vx, vy, vz);
+            const typename Fmt<FMT>::W w = __ldg(Layout<FMT>::weight(m, slot) + li);
+            if (w != 0) {
+                valid = true;
+                return Fmt<FMT>::dq(__ldg(Layout<FMT>::tsdf(m, slot) + li));
+            }
+        }
+        valid = false;
+        return 1.f;
+    }
+
+    // read_sdf_interped (ray_tracing.cu:288-321)
+    __device__ float interp(float3 p, bool& valid)
+    {
+        const float flx = floorf(p.x), fly = floorf(p.y), flz = floorf(p.z);
+        const float ax = __fsub_rn(p.x, flx), ay = __fsub_rn(p.y, fly), az = __fsub_rn(p.z, flz);
+        const int x0 = __float2int_rz(flx), y0 = __float2int_rz(fly), z0 = __float2int_rz(flz);
+        const int x1 = __float2int_rz(floorf(__fadd_rn(p.x, 1.f)));
+        const int y1 = __float2int_rz(floorf(__fadd_rn(p.y, 1.f)));
+        const int z1 = __float2int_rz(floorf(__fadd_rn(p.z, 1.f)));
+        float s[8];
+        bool ok = true;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const int vx = (c & 1) ? x1 : x0, vy = (c & 2) ? y1 : y0, vz = (c & 4) ? z1 : z0;
+            bool v;
+            s[c] = voxel(block_of(vox2blk(vx), vox2blk(vy), vox2blk(vz)), vx, vy, vz, v);
+            ok &= v;
+        }
+        const float bx = __fsub_rn(1.f, ax), by = __fsub_rn(1.f, ay), bz = __fsub_rn(1.f, az);
+        const float r0 = __fmaf_rn(bx, s[0], __fmul_rn(ax, s[1]));
+        const float r1 = __fmaf_rn(bx, s[2], __fmul_rn(ax, s[3]));
+        const float r2 = __fmaf_rn(by, r0, __fmul_rn(ay, r1));
+        const float r4 = __fmaf_rn(bx, s[4], __fmul_rn(ax, s[5]));
+        const float r5 = __fmaf_rn(bx, s[6], __fmul_rn(ax, s[7]));
+        const float r3 = __fmaf_rn(by, r4, __fmul_rn(ay, r5));
+        valid = ok;
+        return __fmaf_rn(bz, r2, __fmul_rn(az, r3));
+    }
+};
+
+__device__ __forceinline__ float3 fma3(float k, float3 d, float3 r)
+{
+    return make_float3(__fmaf_rn(k, d.x, r.x), __fmaf_rn(k, d.y, r.y), __fmaf_rn(k, d.z, r.z));
+}
+
+// MapRenderingDelegate::operator() (ray_tracing.cu:323-400). 8x32-pixel CTAs,
+// each warp an 8x4 pixel tile.
+template <int FMT>
+__global__ void __launch_bounds__(256) raycast_kernel(DevMap m, RenderParams r, float4* vmap, size_t vpitch)
+{
+    const int x = blockIdx.x * 8 + threadIdx.x;
+    const int y = blockIdx.y * 32 + threadIdx.y;
+    if (x >= r.W || y >= r.H) return;
+    float4* out = reinterpret_cast<float4*>(reinterpret_cast<char*>(vmap) + (size_t)y * vpitch) + x;
+    const float qnan = __int_as_float(0x7fffffff);
+    const float4 miss = make_float4(qnan, qnan, qnan, qnan);
+
+    float zn = 0.f, zf = kMaxDepth;
+    if (r.mode == 0) {
+        const int t = (y >> 3) * r.tilesX + (x >> 3);
+        zn = __uint_as_float(r.zmin[t]);
+        zf = __uint_as_float(r.zmax[t]);
+        if (!(zn <= zf)) {  // no allocated block projects into this tile
+            *out = miss;
+            return;
+        }
+    }
+
+    const float3 p0 = unproject(x, y, kMinDepth, r.ifx, r.ify, r.cx, r.cy);
+    const float dist0 = __fmul_rn(__fsqrt_rn(sqnorm(p0)), r.vsinv);
+    float3 bs = xf_apply(r.T, p0.x, p0.y, p0.z);
+    bs = make_float3(__fmul_rn(bs.x, r.vsinv), __fmul_rn(bs.y, r.vsinv), __fmul_rn(bs.z, r.vsinv));
+    const float3 p1 = unproject(x, y, kMaxDepth, r.ifx, r.ify, r.cx, r.cy);
+    const float dist_e = __fmul_rn(__fsqrt_rn(sqnorm(p1)), r.vsinv);
+    float3 be = xf_apply(r.T, p1.x, p1.y, p1.z);
+    be = make_float3(__fmul_rn(be.x, r.vsinv), __fmul_rn(be.y, r.vsinv), __fmul_rn(be.z, r.vsinv));
+    const float3 dir = normalized(make_float3(__fsub_rn(be.x, bs.x), __fsub_rn(be.y, bs.y), __fsub_rn(be.z, bs.z)));
+
+    float3 res = bs;
+    float dist_s = dist0;
+    float dist_lim = dist_e;
+    if (r.mode == 0) {
+        // ray length (voxels) is proportional to camera depth along a ray
+        const float g = dist_e / kMaxDepth;
+        const float k0 = floorf(g * zn - dist0) - 2.f;
+        if (k0 > 0.f) {
+            res = fma3(k0, dir, res);
+            dist_s = dist0 + k0;
+        }
+        dist_lim = fminf(dist_e, g * zf + 2.f);
+    }
+
+    RayCtx<FMT> ctx(m);
+    float sdf = 1.f, step;
+    bool valid = false;
+    while (dist_s < dist_lim) {
+        const float flx = floorf(res.x), fly = floorf(res.y), flz = floorf(res.z);
+        const int vx = __float2int_rz(flx), vy = __float2int_rz(fly), vz = __float2int_rz(flz);
+        const int bx = vox2blk(vx), by = vox2blk(vy), bz = vox2blk(vz);
+        if (bx != ctx.cbx || by != ctx.cby || bz != ctx.cbz) {
+            const int s = (bx == ctx.obx && by == ctx.oby && bz == ctx.obz) ? ctx.oblk : hash_find(m, bx, by, bz);
+            ctx.cbx = bx;
+            ctx.cby = by;
+            ctx.cbz = bz;
+            ctx.cblk = s;
+        }
+        if (ctx.cblk < 0) {
+            // every 1-voxel step inside this unallocated block reads (1.0, invalid):
+            // jump to the last step that is still inside (at least one step)
+            float t = 1e30f;
+            if (dir.x > 0.f) t = fminf(t, ((float)(bx * 8 + 8) - res.x) / dir.x);
+            else if (dir.x < 0.f) t = fminf(t, ((float)(bx * 8) - res.x) / dir.x);
+            if (dir.y > 0.f) t = fminf(t, ((float)(by * 8 + 8) - res.y) / dir.y);
+            else if (dir.y < 0.f) t = fminf(t, ((float)(by * 8) - res.y) / dir.y);
+            if (dir.z > 0.f) t = fminf(t, ((float)(bz * 8 + 8) - res.z) / dir.z);
+            else if (dir.z < 0.f) t = fminf(t, ((float)(bz * 8) - res.z) / dir.z);
+            const float k = fmaxf(1.f, ceilf(t - 1e-3f));
+            res = fma3(k, dir, res);
+            dist_s = __fadd_rn(dist_s, k);
+            sdf = 1.f;
+            valid = false;
+            continue;
+        }
+        sdf = ctx.voxel(ctx.cblk, vx, vy, vz, valid);
+        if (sdf <= 0.5f && sdf >= -0.5f) sdf = ctx.interp(res, valid);
+        if (sdf <= 0.f) break;
+        step = valid ? fmaxf(__fmul_rn(sdf, r.rts), 1.f) : 1.f;
+        res = fma3(step, dir, res);
+        dist_s = __fadd_rn(dist_s, step);
+    }
+
+    bool found = false;
+    if (sdf <= 0.f) {
+        step = __fmul_rn(sdf, r.rts);
+        res = fma3(step, dir, res);
+        sdf = ctx.interp(res, valid);
+        step = __fmul_rn(sdf, r.rts);
+        res = fma3(step, dir, res);
+        found = valid;
+    }
+    if (found) {
+        const float3 o = xf_apply(r.Ti, __fdiv_rn(res.x, r.vsinv), __fdiv_rn(res.y, r.vsinv),
+                                  __fdiv_rn(res.z, r.vsinv));
+        *out = make_float4(o.x, o.y, o.z, 1.f);
+    } else {
+        *out = miss;
+    }
+}
+
+// ------------------------------------------------------------------ normals
+// computeNormalKernel (image_proc.cu:74-93): normalize((v[x+1] - v[x-1]) x
+// (v[y+1] - v[y-1])), w = 1. Undefined pixels (last row / column, NaN
+// neighbour) are written all-NaN.
+__global__ void __launch_bounds__(256) normals_kernel(const float4* vmap, size_t vpitch, float4* nmap,
+                                                      size_t npitch, int W, int H)
+{
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= W || y >= H) return;
+    const float qnan = __int_as_float(0x7fffffff);
+    float4 res = make_float4(qnan, qnan, qnan, qnan);
+    if (x < W - 1 && y < H - 1) {
+        auto at = [&](int xx, int yy) {
+            return __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(vmap) + (size_t)yy * vpitch) + xx);
+        };
+        const float4 v00 = at(max(x - 1, 0), y), v01 = at(x + 1, y), v10 = at(x, max(y - 1, 0)), v11 = at(x, y + 1);
+        if (!(isnan(v00.x) || isnan(v01.x) || isnan(v10.x) || isnan(v11.x))) {
+            const float3 a = make_float3(__fsub_rn(v01.x, v00.x), __fsub_rn(v01.y, v00.y), __fsub_rn(v01.z, v00.z));
+            const float3 b = make_float3(__fsub_rn(v11.x, v10.x), __fsub_rn(v11.y, v10.y), __fsub_rn(v11.z, v10.z));
+            const float3 n = normalized(cross3(a, b));
+            res = make_float4(n.x, n.y, n.z, 1.f);
+        }
+    }
+    *(reinterpret_cast<float4*>(reinterpret_cast<char*>(nmap) + (size_t)y * npitch) + x) = res;
+}
+
+// -------------------------------------------------------------------- Phong
+// renderPoint (image_proc.cu:8-44): light at (5,5,5), Ka 0.3, Kd 0.5, Ks 0.2,
+// exponent 20, unit material colour; background (4,2,2)/255.
+__global__ void __launch_bounds__(256) phong_kernel(const float4* vmap, size_t vpitch, const float4* nmap,
+                                                    size_t npitch, uchar4* rgba, size_t rpitch, int W, int H)
+{
+    const int x = blockIdx.x * 32 + (threadIdx.x & 31);
+    const int y = blockIdx.y * 8 + (threadIdx.x >> 5);
+    if (x >= W || y >= H) return;
+    const float4 p = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(vmap) + (size_t)y * vpitch) + x);
+    const float4 n = __ldg(reinterpret_cast<const float4*>(reinterpret_cast<const char*>(nmap) + (size_t)y * npitch) + x);
+    float c0 = 4.f / 255.f, c1 = 2.f / 255.f, c2 = 2.f / 255.f;
+    if (!isnan(p.x)) {
+        const float3 L = normalized(make_float3(__fsub_rn(5.f, p.x), __fsub_rn(5.f, p.y), __fsub_rn(5.f, p.z)));
+        const float3 V = normalized(make_float3(__fsub_rn(0.f, p.x), __fsub_rn(0.f, p.y), __fsub_rn(0.f, p.z)));
+        const float nl = __fmaf_rn(n.x, L.x, __fmaf_rn(n.y, L.y, __fmul_rn(n.z, L.z)));
+        const float3 R = normalized(make_float3(__fmaf_rn(__fmul_rn(2.f, n.x), nl, -L.x),
+                                                __fmaf_rn(__fmul_rn(2.f, n.y), nl, -L.y),
+                                                __fmaf_rn(__fmul_rn(2.f, n.z), nl, -L.z)));
+        const float rv = __fmaf_rn(R.x, V.x, __fmaf_rn(R.y, V.y, __fmul_rn(R.z, V.z)));
+        const float I = __fmaf_rn(0.2f, powf(fmaxf(0.f, rv), 20.f), __fmaf_rn(0.5f, fmaxf(0.f, nl), 0.3f));
+        c0 = c1 = c2 = I;
+    }
+    uchar4 o;
+    o.x = (unsigned char)__float2uint_rz(__saturatef(c0) * 255.f);
+    o.y = (unsigned char)__float2uint_rz(__saturatef(c1) * 255.f);
+    o.z = (unsigned char)__float2uint_rz(__saturatef(c2) * 255.f);
+    o.w = 255;
+    *(reinterpret_cast<uchar4*>(reinterpret_cast<char*>(rgba) + (size_t)y * rpitch) + x) = o;
+}
+
+// ------------------------------------------------------------------ launchers
+cudaError_t launch_zrange(const DevMap& m, const RenderParams& r, const Launcher& l, cudaStream_t s)
+{
+    const size_t nt = (size_t)r.tilesX * r.tilesY * sizeof(unsigned);
+    cudaError_t e = cudaMemsetAsync(r.zmin, 0x7f, nt, s);  // 0x7f7f7f7f = 3.4e38f
+    if (e != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(r.zmax, 0, nt, s)) != cudaSuccess) return e;
+    zrange_kernel<<<l.numSMs * 4, 256, 0, s>>>(m, r);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_raycast(const DevMap& m, int fmt, const RenderParams& r, float4* vmap, size_t vpitch,
+                           const Launcher&, cudaStream_t s)
+{
+    dim3 block(8, 32), grid((r.W + 7) / 8, (r.H + 31) / 32);
+    switch (fmt) {
+    case VMAP_VOXEL_REF: raycast_kernel<VMAP_VOXEL_REF><<<grid, block, 0, s>>>(m, r, vmap, vpitch); break;
+    case VMAP_VOXEL_F32: raycast_kernel<VMAP_VOXEL_F32><<<grid, block, 0, s>>>(m, r, vmap, vpitch); break;
+    case VMAP_VOXEL_F16: raycast_kernel<VMAP_VOXEL_F16><<<grid, block, 0, s>>>(m, r, vmap, vpitch); break;
+    case VMAP_VOXEL_I16: raycast_kernel<VMAP_VOXEL_I16><<<grid, block, 0, s>>>(m, r, vmap, vpitch); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_normals(const float4* vmap, size_t vpitch, float4* nmap, size_t npitch, int W, int H,
+                           cudaStream_t s)
+{
+    dim3 grid((W + 31) / 32, (H + 7) / 8);
+    normals_kernel<<<grid, 256, 0, s>>>(vmap, vpitch, nmap, npitch, W, H);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_phong(const float4* vmap, size_t vpitch, const float4* nmap, size_t npitch, uchar4* rgba,
+                         size_t rpitch, int W, int H, cudaStream_t s)
+{
+    dim3 grid((W + 31) / 32, (H + 7) / 8);
+    phong_kernel<<<grid, 256, 0, s>>>(vmap, vpitch, nmap, npitch, rgba, rpitch, W, H);
+    return cudaGetLastError();
+}
+
+}  // namespace vmapb

@@ -1,0 +1,332 @@
+// Device-side building blocks shared by the kernels of libvmap_b200.
+//
+// Floating-point policy: every operation whose rounding decides a result that
+// must match the reference's algorithm bit for bit (block coordinates,
+// visibility, projective TSDF updates, marching-cubes vertices) is written
+// with explicit round-to-nearest intrinsics (__fmul_rn, __fadd_rn, __fmaf_rn,
+// __fdiv_rn, __fsqrt_rn). The compiler never contracts or reorders those, so
+// the FP32 operation sequence is the one documented beside each helper: the
+// reference's Eigen expression with nvcc's default multiply-add contraction.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <cooperative_groups.h>
+#include <stdint.h>
+
+#include "../../include/vmap_c.h"
+
+namespace vmapb {
+
+namespace cg = cooperative_groups;
+
+// Reference constants (include/map_struct.h:6-10).
+constexpr int kBlockSide = 8;
+constexpr int kBlockVoxels = 512;
+constexpr float kMinDepth = 0.1f;
+constexpr float kMaxDepth = 5.f;
+// Slots per hash bucket: four 64-bit keys = one 32-byte L2 sector per probe.
+constexpr int kSlots = 4;
+constexpr int kMaxProbe = 64;  // buckets visited before VMAP_FLAG_HASH_FULL
+constexpr unsigned long long kEmptyKey = ~0ull;
+constexpr int kCoordLimit = 1 << 20;  // block coordinates in [-2^20, 2^20)
+constexpr int kZTile = 8;             // z-range tile edge (reference SubSample 8)
+
+// device counters (uint32 array in device memory)
+enum {
+    C_ALLOC = 0,   // pool bump pointer (may run past capacity on failure)
+    C_VISIBLE = 1, // visible blocks of the last selection
+    C_ERR = 2,     // VMAP_FLAG_* bits
+    C_TRI = 3,     // triangles counted by the last polygonize
+    C_FAILED = 4,  // allocations refused (pool full)
+    C_COUNT = 16
+};
+
+// 3x4 affine transform, row-major; passed by value as a kernel argument.
+struct Xf {
+    float m[3][4];
+};
+
+struct DevMap {
+    unsigned long long* keys;      // nBucket * kSlots packed block coordinates
+    int* vals;                     // nBucket * kSlots pool slot (or -1)
+    unsigned long long* blockKeys; // capacity: key of each allocated block
+    unsigned char* pool;           // capacity * blockBytes
+    unsigned* ctr;                 // C_COUNT counters
+    int* visList;                  // capacity: visible block slots
+    int nBucket;
+    int capacity;
+    int blockBytes;
+    float vs;   // voxel size
+    float mu;   // truncation distance
+    float wmax; // weight cap
+};
+
+// ---------------------------------------------------------------- FP32 math
+// Transform<float,3,Affine> * Vector3f (map_struct.h:201,212):
+// t_i + (m_i0 v0 + (m_i1 v1 + m_i2 v2)), each product contracted into its add.
+__device__ __forceinline__ float3 xf_apply(const Xf& t, float v0, float v1, float v2)
+{
+    float3 o;
+    o.x = __fadd_rn(t.m[0][3], __fmaf_rn(t.m[0][0], v0, __fmaf_rn(t.m[0][1], v1, __fmul_rn(t.m[0][2], v2))));
+    o.y = __fadd_rn(t.m[1][3], __fmaf_rn(t.m[1][0], v0, __fmaf_rn(t.m[1][1], v1, __fmul_rn(t.m[1][2], v2))));
+    o.z = __fadd_rn(t.m[2][3], __fmaf_rn(t.m[2][0], v0, __fmaf_rn(t.m[2][1], v1, __fmul_rn(t.m[2][2], v2))));
+    return o;
+}
+
+// unproject (map_struct.h:189-194): ((ifx * (x - cx)) * z, (ify * (y - cy)) * z, z)
+__device__ __forceinline__ float3 unproject(int x, int y, float z, float ifx, float ify, float cx, float cy)
+{
+    return make_float3(__fmul_rn(__fmul_rn(ifx, __fsub_rn(__int2float_rn(x), cx)), z),
+                       __fmul_rn(__fmul_rn(ify, __fsub_rn(__int2float_rn(y), cy)), z), z);
+}
+
+// Eigen squaredNorm: v0^2 + (v1^2 + v2^2), contracted.
+__device__ __forceinline__ float sqnorm(float3 v)
+{
+    return __fmaf_rn(v.x, v.x, __fmaf_rn(v.y, v.y, __fmul_rn(v.z, v.z)));
+}
+
+// Eigen normalized(): v / sqrt(|v|^2) if |v|^2 > 0 else v.
+__device__ __forceinline__ float3 normalized(float3 v)
+{
+    const float s = sqnorm(v);
+    if (s > 0.f) {
+        const float n = __fsqrt_rn(s);
+        v.x = __fdiv_rn(v.x, n);
+        v.y = __fdiv_rn(v.y, n);
+        v.z = __fdiv_rn(v.z, n);
+    }
+    return v;
+}
+
+// Eigen cross(): a1 b2 - a2 b1, ... contracted as fma(a1, b2, -(a2 b1)).
+__device__ __forceinline__ float3 cross3(float3 a, float3 b)
+{
+    return make_float3(__fmaf_rn(a.y, b.z, -__fmul_rn(a.z, b.y)), __fmaf_rn(a.z, b.x, -__fmul_rn(a.x, b.z)),
+                       __fmaf_rn(a.x, b.y, -__fmul_rn(a.y, b.x)));
+}
+
+// ------------------------------------------------------- coordinate helpers
+// voxelPosToBlockPos (map_struct.h:131-141) == floor division by 8.
+__device__ __forceinline__ int vox2blk(int v) { return v >> 3; }
+// localPosToLocalIdx(voxelPosToLocalPos(v)) (map_struct.h:148-180).
+__device__ __forceinline__ int local_idx(int vx, int vy, int vz)
+{
+    return ((vz & 7) << 6) | ((vy & 7) << 3) | (vx & 7);
+}
+
+__device__ __forceinline__ bool coord_ok(int x, int y, int z)
+{
+    return x >= -kCoordLimit && x < kCoordLimit && y >= -kCoordLimit && y < kCoordLimit && z >= -kCoordLimit &&
+           z < kCoordLimit;
+}
+
+__device__ __forceinline__ unsigned long long pack_key(int x, int y, int z)
+{
+    return ((unsigned long long)(x & 0x1FFFFF) << 42) | ((unsigned long long)(y & 0x1FFFFF) << 21) |
+           (unsigned long long)(z & 0x1FFFFF);
+}
+
+__device__ __forceinline__ int3 unpack_key(unsigned long long k)
+{
+    return make_int3((int)((long long)(k << 1) >> 43), (int)((long long)(k << 22) >> 43),
+                     (int)((long long)(k << 43) >> 43));
+}
+
+// hash (map_struct.h:104-109): int32 wrap-around products, C remainder,
+// shifted non-negative.
+__device__ __forceinline__ int ref_hash(int x, int y, int z, int nb)
+{
+    int r = (int)(((unsigned)x * 73856093u) ^ ((unsigned)y * 19349669u) ^ ((unsigned)z * 83492791u));
+    r %= nb;
+    return r < 0 ? r + nb : r;
+}
+
+// checkBlockVisible (map_struct.h:219-244): any of the 8 block corners
+// projects inside [0, cols-1] x [0, rows-1] with depth in [0.1, 5].
+__device__ __forceinline__ bool block_visible(int bx, int by, int bz, const Xf& ti, float scale, int cols,
+                                              int rows, float fx, float fy, float cx, float cy)
+{
+    const float cmax = __int2float_rn(cols - 1), rmax = __int2float_rn(rows - 1);
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        const float3 p = xf_apply(ti, __fmul_rn(__int2float_rn(bx + (c & 1)), scale),
+                                  __fmul_rn(__int2float_rn(by + ((c >> 1) & 1)), scale),
+                                  __fmul_rn(__int2float_rn(bz + ((c >> 2) & 1)), scale));
+        const float px = __fadd_rn(__fdiv_rn(__fmul_rn(fx, p.x), p.z), cx);
+        const float py = __fadd_rn(__fdiv_rn(__fmul_rn(fy, p.y), p.z), cy);
+        if (!(px < 0.f || py < 0.f || px > cmax || py > rmax || p.z < kMinDepth || p.z > kMaxDepth)) return true;
+    }
+    return false;
+}
+
+// ------------------------------------------------------------- hash table
+// Bucketed open hashing: bucket = reference hash of the block coordinates,
+// 4 slots per bucket (one 32-byte sector), linear probing into the next
+// bucket when all 4 are taken. Slots go EMPTY -> key exactly once, so the
+// filled slots of a bucket always form a prefix: a lookup stops at the first
+// EMPTY slot.
+__device__ __forceinline__ int hash_find(const DevMap& m, int bx, int by, int bz)
+{
+    if (!coord_ok(bx, by, bz)) return -1;
+    const unsigned long long key = pack_key(bx, by, bz);
+    int b = ref_hash(bx, by, bz, m.nBucket);
+#pragma unroll 1
+    for (int p = 0; p < kMaxProbe; ++p) {
+        const ulonglong2* s = reinterpret_cast<const ulonglong2*>(m.keys + (size_t)b * kSlots);
+        const ulonglong2 k01 = __ldg(s), k23 = __ldg(s + 1);
+        const int base = b * kSlots;
+        if (k01.x == key) return __ldg(m.vals + base);
+        if (k01.x == kEmptyKey) return -1;
+        if (k01.y == key) return __ldg(m.vals + base + 1);
+        if (k01.y == kEmptyKey) return -1;
+        if (k23.x == key) return __ldg(m.vals + base + 2);
+        if (k23.x == kEmptyKey) return -1;
+        if (k23.y == key) return __ldg(m.vals + base + 3);
+        if (k23.y == kEmptyKey) return -1;
+        b = (b + 1 == m.nBucket) ? 0 : b + 1;
+    }
+    return -1;
+}
+
+// Insert a block if absent (createBlock, map_struct.h:304-354, without its
+// lock: a compare-and-swap claims an empty slot, losers re-read). The winner
+// takes the next pool slot from a warp-aggregated bump counter, which hands
+// out blocks in the reference's heap order 0, 1, 2, ...
+__device__ __forceinline__ void hash_insert(const DevMap& m, int bx, int by, int bz)
+{
+    const unsigned long long key = pack_key(bx, by, bz);
+    int b = ref_hash(bx, by, bz, m.nBucket);
+#pragma unroll 1
+    for (int p = 0; p < kMaxProbe; ++p) {
+        unsigned long long* s = m.keys + (size_t)b * kSlots;
+        const ulonglong2 k01 = __ldcg(reinterpret_cast<const ulonglong2*>(s));
+        const ulonglong2 k23 = __ldcg(reinterpret_cast<const ulonglong2*>(s) + 1);
+        const unsigned long long k[4] = {k01.x, k01.y, k23.x, k23.y};
+#pragma unroll
+        for (int i = 0; i < kSlots; ++i) {
+            unsigned long long cur = k[i];
+            if (cur == kEmptyKey) cur = atomicCAS(s + i, kEmptyKey, key);
+            if (cur == key) return;  // present (or inserted by another thread)
+            if (cur == kEmptyKey) {  // this thread won the slot
+                cg::coalesced_group g = cg::coalesced_threads();
+                unsigned first = 0;
+                if (g.thread_rank() == 0) first = atomicAdd(m.ctr + C_ALLOC, g.size());
+                const unsigned slot = g.shfl(first, 0) + g.thread_rank();
+                if (slot < (unsigned)m.capacity) {
+                    m.blockKeys[slot] = key;
+                    m.vals[(size_t)b * kSlots + i] = (int)slot;
+                } else {
+                    atomicOr(m.ctr + C_ERR, VMAP_FLAG_POOL_FULL);
+                    atomicAdd(m.ctr + C_FAILED, 1u);
+                }
+                return;
+            }
+        }
+        b = (b + 1 == m.nBucket) ? 0 : b + 1;
+    }
+    atomicOr(m.ctr + C_ERR, VMAP_FLAG_HASH_FULL);
+}
+
+__device__ __forceinline__ int allocated_blocks(const DevMap& m)
+{
+    const unsigned n = *((volatile const unsigned*)(m.ctr + C_ALLOC));
+    return n < (unsigned)m.capacity ? (int)n : m.capacity;
+}
+
+// ------------------------------------------------------------ voxel formats
+// Per-block plane layout: [tsdf x512][weight x512][r x512][g x512][b x512].
+template <int FMT>
+struct Fmt;
+
+template <>
+struct Fmt<VMAP_VOXEL_REF> {  // reference Voxel: int16 x32767, uint8 weight
+    typedef short T;
+    typedef unsigned char W;
+    // unpackFloat (map_struct.h:72-75): val / 32767.f
+    static __device__ __forceinline__ float dq(T c) { return __fdiv_rn(__int2float_rn(c), 32767.f); }
+    // packFloat (map_struct.h:77-80): (short)(val * 32767), truncation
+    static __device__ __forceinline__ T q(float v) { return (short)__float2int_rz(__fmul_rn(v, 32767.f)); }
+    static __device__ __forceinline__ float wf(W w) { return (float)w; }
+    static __device__ __forceinline__ W wq(float w) { return (W)__float2uint_rz(w); }
+};
+
+template <>
+struct Fmt<VMAP_VOXEL_F32> {
+    typedef float T;
+    typedef float W;
+    static __device__ __forceinline__ float dq(T c) { return c; }
+    static __device__ __forceinline__ T q(float v) { return v; }
+    static __device__ __forceinline__ float wf(W w) { return w; }
+    static __device__ __forceinline__ W wq(float w) { return w; }
+};
+
+template <>
+struct Fmt<VMAP_VOXEL_F16> {
+    typedef unsigned short T;  // IEEE half bits
+    typedef unsigned short W;
+    static __device__ __forceinline__ float dq(T c) { return __half2float(__ushort_as_half(c)); }
+    static __device__ __forceinline__ T q(float v) { return __half_as_ushort(__float2half_rn(v)); }
+    static __device__ __forceinline__ float wf(W w) { return (float)w; }
+    static __device__ __forceinline__ W wq(float w) { return (W)__float2uint_rz(w); }
+};
+
+template <>
+struct Fmt<VMAP_VOXEL_I16> {
+    typedef short T;
+    typedef unsigned short W;
+    static __device__ __forceinline__ float dq(T c) { return __fdiv_rn(__int2float_rn(c), 32767.f); }
+    static __device__ __forceinline__ T q(float v) { return (short)__float2int_rz(__fmul_rn(v, 32767.f)); }
+    static __device__ __forceinline__ float wf(W w) { return (float)w; }
+    static __device__ __forceinline__ W wq(float w) { return (W)__float2uint_rz(w); }
+};
+
+template <int FMT>
+struct Layout {
+    typedef typename Fmt<FMT>::T T;
+    typedef typename Fmt<FMT>::W W;
+    static constexpr int kTsdfOff = 0;
+    static constexpr int kWOff = kBlockVoxels * (int)sizeof(T);
+    static constexpr int kRgbOff = kBlockVoxels * (int)(sizeof(T) + sizeof(W));
+    static __host__ __device__ constexpr int bytes(bool color)
+    {
+        return kBlockVoxels * (int)(sizeof(T) + sizeof(W)) + (color ? 3 * kBlockVoxels : 0);
+    }
+    static __device__ __forceinline__ const T* tsdf(const DevMap& m, int slot)
+    {
+        return reinterpret_cast<const T*>(m.pool + (size_t)slot * m.blockBytes + kTsdfOff);
+    }
+    static __device__ __forceinline__ const W* weight(const DevMap& m, int slot)
+    {
+        return reinterpret_cast<const W*>(m.pool + (size_t)slot * m.blockBytes + kWOff);
+    }
+};
+
+// 16-byte vectorised copies of a row of 8 voxels.
+template <int NBYTES>
+__device__ __forceinline__ void load_row(const void* src, void* dst)
+{
+    static_assert(NBYTES == 8 || NBYTES % 16 == 0, "row size");
+    if constexpr (NBYTES == 8) {
+        *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
+    } else {
+#pragma unroll
+        for (int i = 0; i < NBYTES / 16; ++i)
+            reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+    }
+}
+
+template <int NBYTES>
+__device__ __forceinline__ void store_row(void* dst, const void* src)
+{
+    if constexpr (NBYTES == 8) {
+        *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
+    } else {
+#pragma unroll
+        for (int i = 0; i < NBYTES / 16; ++i)
+            reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
+    }
+}
+
+}  // namespace vmapb

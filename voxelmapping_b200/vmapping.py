@@ -1,0 +1,188 @@
+"""Python mirror of the reference's ``vmap::VoxelMapping`` class.
+
+Same methods, argument meaning and ownership as include/vmapping.h:10-27 of
+xingruiyang/VoxelMapping (whose Python bindings live in an external project),
+implemented over the C ABI of libvmap_b200.so. Device images are torch CUDA
+tensors (torch is only the device-memory and stream plumbing); host images are
+numpy arrays.
+
+    vm = VoxelMapping(640, 480, K)
+    vm.CreateMap(numEntries=1 << 21, numVoxels=1 << 20, voxelSize=0.005)
+    vm.FuseDepth(depth_cuda, camToWorld)           # float metres (h, w)
+    vmap = vm.RenderScene(None, camToWorld)        # (h, w, 4) camera-frame vertices
+    n, verts, norms = vm.Polygonize()              # reference: int + two float* (9 per triangle)
+
+Differences from the reference, by design: errors raise VmapError instead of
+exit(0); FuseDepthAndImage is implemented (a stub in the reference,
+vmapping.cpp:167-170); misses in the vertex map are NaN in all four lanes.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+
+
+def _stream():
+    import torch
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+class VoxelMapping:
+    def __init__(self, w, h, K, voxel_format="f32", with_color=True, max_weight=0, truncation=0.0,
+                 raycast_mode=0, num_buckets=0):
+        self.width, self.height = int(w), int(h)
+        self.K = np.asarray(K, dtype=np.float64).reshape(3, 3)
+        self.voxel_format = L.FORMAT_NAMES[voxel_format] if isinstance(voxel_format, str) else int(voxel_format)
+        self.with_color = bool(with_color)
+        self.max_weight = int(max_weight)
+        self.truncation = float(truncation)
+        self.raycast_mode = int(raycast_mode)
+        self.num_buckets = int(num_buckets)
+        self._map = None
+        self._lib = L.lib()
+
+    # -- lifetime ------------------------------------------------------------
+    def CreateMap(self, numEntries, numVoxels, voxelSize):
+        """vmapping.cpp:57-75: allocate and reset the map."""
+        self.release()
+        cfg = L.Config(self.width, self.height, float(self.K[0, 0]), float(self.K[1, 1]), float(self.K[0, 2]),
+                       float(self.K[1, 2]), int(numEntries), int(numVoxels), float(voxelSize), self.num_buckets,
+                       self.truncation, self.voxel_format, self.max_weight, int(self.with_color), self.raycast_mode)
+        h = C.c_void_p()
+        L.check(self._lib.vmap_create(C.byref(cfg), C.byref(h)), "vmap_create")
+        self._map = h
+        self.config = self.get_config()
+
+    def release(self):
+        if self._map is not None:
+            L.check(self._lib.vmap_destroy(self._map), "vmap_destroy")
+            self._map = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def reset(self):
+        L.check(self._lib.vmap_reset(self._need(), _stream()), "vmap_reset")
+
+    def _need(self):
+        if self._map is None:
+            raise L.VmapError(1, "map not created (call CreateMap first)")
+        return self._map
+
+    def get_config(self):
+        cfg = L.Config()
+        L.check(self._lib.vmap_get_config(self._need(), C.byref(cfg)), "vmap_get_config")
+        return {k: getattr(cfg, k) for k, _ in cfg._fields_}
+
+    # -- fusion --------------------------------------------------------------
+    def FuseDepth(self, depth, camToWorld, depth_scale=0.001):
+        """Fuse a device depth image: float32 metres or uint16 (x depth_scale)."""
+        import torch
+        assert depth.is_cuda and depth.shape[-2:] == (self.height, self.width)
+        dt = L.DEPTH_U16 if depth.dtype in (torch.uint16, torch.int16) else L.DEPTH_F32
+        if dt == L.DEPTH_F32:
+            assert depth.dtype == torch.float32
+        L.check(self._lib.vmap_fuse_depth(self._need(), _ptr(depth), dt, depth.stride(0) * depth.element_size(),
+                                          depth_scale, L.pose_arg(camToWorld), _stream()), "vmap_fuse_depth")
+
+    def FuseDepthAndImage(self, rgb, depth, camToWorld, depth_scale=0.001):
+        """Fuse depth + uint8x3 colour. numpy inputs take the host-buffer path
+        (the reference signature takes cv::Mat), torch CUDA tensors the device path."""
+        m = self._need()
+        if isinstance(depth, np.ndarray):
+            depth = np.ascontiguousarray(depth)
+            rgb_p = None
+            if rgb is not None:
+                rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+                rgb_p = rgb.ctypes.data_as(C.c_void_p)
+            dt = L.DEPTH_U16 if depth.dtype == np.uint16 else L.DEPTH_F32
+            if dt == L.DEPTH_F32:
+                depth = depth.astype(np.float32, copy=False)
+            L.check(self._lib.vmap_fuse_host(m, depth.ctypes.data_as(C.c_void_p), dt, depth_scale, rgb_p,
+                                             L.pose_arg(camToWorld), _stream()), "vmap_fuse_host")
+            import torch
+            torch.cuda.current_stream().synchronize()  # host buffers may be pageable and reused
+            return
+        import torch
+        dt = L.DEPTH_U16 if depth.dtype in (torch.uint16, torch.int16) else L.DEPTH_F32
+        L.check(self._lib.vmap_fuse_depth_rgb(m, _ptr(depth), dt, depth.stride(0) * depth.element_size(),
+                                              depth_scale, _ptr(rgb), rgb.stride(0), L.pose_arg(camToWorld),
+                                              _stream()), "vmap_fuse_depth_rgb")
+
+    def CheckVisibleBlocks(self, camToWorld):
+        L.check(self._lib.vmap_check_visible_blocks(self._need(), L.pose_arg(camToWorld), _stream()))
+        return self.stats()["visible_blocks"]
+
+    # -- raycast -------------------------------------------------------------
+    def RenderScene(self, vmap, camToWorld, nmap=None):
+        """Raycast the map at camToWorld into vmap ((h, w, 4) float32 CUDA,
+        allocated when None); nmap receives normals when given. Returns vmap."""
+        import torch
+        if vmap is None:
+            vmap = torch.empty((self.height, self.width, 4), dtype=torch.float32, device="cuda")
+        L.check(self._lib.vmap_render_scene(self._need(), L.pose_arg(camToWorld), _ptr(vmap), vmap.stride(0) * 4,
+                                            _ptr(nmap) if nmap is not None else None,
+                                            nmap.stride(0) * 4 if nmap is not None else 0, _stream()),
+                "vmap_render_scene")
+        return vmap
+
+    # -- meshing -------------------------------------------------------------
+    def Polygonize(self):
+        """Returns (num_triangles, verts, norms): (n, 9) float32 arrays copied
+        from the library-owned host buffers (reference: int + float*&)."""
+        vp, np_ = C.POINTER(C.c_float)(), C.POINTER(C.c_float)()
+        n = C.c_uint32()
+        L.check(self._lib.vmap_polygonize_host(self._need(), C.byref(vp), C.byref(np_), C.byref(n), _stream()),
+                "vmap_polygonize_host")
+        k = n.value
+        if k == 0:
+            return 0, np.zeros((0, 9), np.float32), np.zeros((0, 9), np.float32)
+        verts = np.ctypeslib.as_array(vp, shape=(k, 9)).copy()
+        norms = np.ctypeslib.as_array(np_, shape=(k, 9)).copy()
+        return k, verts, norms
+
+    def GetSurfacePoints(self):
+        """Triangle centroids, (n, 3) float32 (vmapping.cpp:134-147)."""
+        import torch
+        cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+        L.check(self._lib.vmap_polygonize(self._need(), None, None, 0, _ptr(cnt), _stream()))
+        k = int(cnt.item())
+        if k == 0:
+            return np.zeros((0, 3), np.float32)
+        verts = torch.empty((k, 9), dtype=torch.float32, device="cuda")
+        L.check(self._lib.vmap_polygonize(self._map, _ptr(verts), None, k, _ptr(cnt), _stream()))
+        pts = torch.empty((k, 3), dtype=torch.float32, device="cuda")
+        L.check(self._lib.vmap_surface_points(_ptr(verts), k, _ptr(pts), _stream()))
+        return pts.cpu().numpy()
+
+    # -- inspection ----------------------------------------------------------
+    def stats(self):
+        s = L.Stats()
+        L.check(self._lib.vmap_get_stats(self._need(), _stream(), C.byref(s)), "vmap_get_stats")
+        return s.as_dict()
+
+    def clear_errors(self):
+        L.check(self._lib.vmap_clear_errors(self._need(), _stream()))
+
+    def export_blocks(self, with_rgb=None):
+        """Allocated blocks in pool order: coords (n, 3) int32, tsdf / weight
+        (n, 512) float32 (voxel x + 8y + 64z), rgb (n, 512, 3) uint8 or None."""
+        n = self.stats()["allocated_blocks"]
+        with_rgb = self.with_color if with_rgb is None else with_rgb
+        coords = np.zeros((n, 3), np.int32)
+        tsdf = np.zeros((n, 512), np.float32)
+        weight = np.zeros((n, 512), np.float32)
+        rgb = np.zeros((n, 512, 3), np.uint8) if with_rgb else None
+        got = C.c_uint32()
+        cp = lambda a: a.ctypes.data_as(C.c_void_p) if a is not None else None
+        L.check(self._lib.vmap_export_blocks(self._map, cp(coords), cp(tsdf), cp(weight), cp(rgb), n,
+                                             C.byref(got), _stream()), "vmap_export_blocks")
+        return {"coords": coords, "tsdf": tsdf, "weight": weight, "rgb": rgb}
