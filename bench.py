@@ -43,6 +43,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--num-blocks", type=int, default=0, help="override the block pool (small profiling runs)")
     return p.parse_args()
 
 
@@ -111,6 +112,14 @@ class ClockSampler:
 
 
 def gpu_index(local_rank):
+    """nvidia-smi id of this rank's GPU: its UUID (robust to device remapping)."""
+    try:
+        import torch
+        u = str(torch.cuda.get_device_properties(local_rank).uuid)
+        if u:
+            return u if u.startswith("GPU-") else "GPU-" + u
+    except Exception:
+        pass
     vis = os.environ.get("CUDA_VISIBLE_DEVICES")
     if vis:
         ids = [v.strip() for v in vis.split(",") if v.strip()]
@@ -184,6 +193,8 @@ def run_product(args):
     dev = torch.device("cuda", local)
     wl = synth.WORKLOADS[WORKLOAD]
     import dataclasses
+    if args.num_blocks:
+        wl = dataclasses.replace(wl, num_blocks=args.num_blocks)
     wl_r = dataclasses.replace(wl, seed=wl.seed + rank)
     scene = synth.Scene(wl_r)
     nfr = args.warmup + args.steps

@@ -75,10 +75,10 @@ typedef struct vmap_config {
     /* map: reference CreateMap(int numEntries, int numVoxels, float voxelSize) */
     int num_entries;          /* hash entries requested (>= 0; must fit 4 * num_buckets) */
     int num_blocks;           /* voxel-block pool capacity ("numVoxels")        */
-    float voxel_size;         /* metres                                         */
+    float voxel_size;         /* metres, >= 1e-4                                */
     /* extensions (0 selects the reference default) */
     int num_buckets;          /* 0: int(0.9 * num_blocks) as the reference       */
-    float truncation;         /* 0: 4 * voxel_size                              */
+    float truncation;         /* 0: 4 * voxel_size; at most 1024 * voxel_size   */
     int voxel_format;         /* vmap_voxel_format                              */
     int max_weight;           /* 0: 255                                         */
     int with_color;           /* keep uint8x3 colour per voxel                  */

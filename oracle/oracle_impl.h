@@ -165,6 +165,12 @@ static int FN(allocate)(orc_map* m, const float* depth, const double pose[16], i
             FN(unproject)(x, y, df, ifx, ify, cx, cy, u);
             FN(xform_pt)(&T, u, w);
             for (int i = 0; i < 3; ++i) pf[i] = R2I_RZ(FLOOR(w[i] / vs));
+            /* end points outside +-2^23 voxels (+-2^20 blocks): the product
+             * cannot key such blocks and skips the pixel; so does the oracle */
+            int out_of_range = 0;
+            for (int i = 0; i < 3; ++i)
+                out_of_range |= pn[i] < -(1 << 23) || pn[i] >= (1 << 23) || pf[i] < -(1 << 23) || pf[i] >= (1 << 23);
+            if (out_of_range) continue;
             R dir[3] = {(R)(pf[0] - pn[0]), (R)(pf[1] - pn[1]), (R)(pf[2] - pn[2])};
             const R len = SQRT(FN(sqnorm)(dir));
             const int nsteps = (int)ceil(2.0 * (double)len);

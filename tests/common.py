@@ -12,14 +12,14 @@ def block_keys(coords):
 
 
 def make_pair(wl, fmt="ref", color=False, num_blocks=None, raycast_mode=0, max_weight=255, num_buckets=0,
-              width=None, height=None, K=None):
+              width=None, height=None, K=None, num_entries=None):
     w = width or wl.width
     h = height or wl.height
     K = wl.K if K is None else K
     nb = num_blocks or wl.num_blocks
     vm = VoxelMapping(w, h, K, voxel_format=fmt, with_color=color, max_weight=max_weight,
                       raycast_mode=raycast_mode, num_buckets=num_buckets)
-    vm.CreateMap(wl.num_entries, nb, wl.voxel_size)
+    vm.CreateMap(wl.num_entries if num_entries is None else num_entries, nb, wl.voxel_size)
     om = O.OracleMap(w, h, K, nb, wl.voxel_size, storage=fmt, max_weight=max_weight, with_color=color)
     return vm, om
 

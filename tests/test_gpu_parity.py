@@ -69,7 +69,7 @@ def test_block_set_exact_full_size(full_scene):
     vm, om = make_pair(FULL, fmt="f32", color=True)
     d, rgb, pose = full_scene.render(0)
     st, orc = fuse_both(vm, om, d, rgb, pose)
-    assert st["allocated_blocks"] == om.num_blocks() > 10000
+    assert st["allocated_blocks"] == om.num_blocks() > 5000
     assert st["visible_blocks"] == orc["visible"]
     assert_maps_equal(vm, om, color=True)
 
@@ -138,7 +138,7 @@ def test_pool_exhaustion_reports_and_keeps_valid_subset(small_scene):
 
 
 def test_hash_full_flag():
-    vm, _ = make_pair(SMALL, num_buckets=2)
+    vm, _ = make_pair(SMALL, num_buckets=2, num_entries=8)
     d, _, pose = synth.Scene(SMALL).render(0)
     vm.FuseDepth(to_gpu_depth(d), pose)
     st = vm.stats()

@@ -54,17 +54,25 @@ __global__ void __launch_bounds__(256) alloc_kernel(DevMap m, FrameParams f)
                 const int fx = __float2int_rz(floorf(__fdiv_rn(wb.x, m.vs)));
                 const int fy = __float2int_rz(floorf(__fdiv_rn(wb.y, m.vs)));
                 const int fz = __float2int_rz(floorf(__fdiv_rn(wb.z, m.vs)));
-                float3 dir = make_float3(__int2float_rn(fx - nx), __int2float_rn(fy - ny), __int2float_rn(fz - nz));
-                const float len = __fsqrt_rn(sqnorm(dir));
-                // (int)ceil(2.0 * len): the double product of a float by 2 is exact
-                n = __float2int_rz(ceilf(__fmul_rn(2.f, len)));
-                const float den = __int2float_rn(n - 1);
-                dx = __fdiv_rn(dir.x, den);
-                dy = __fdiv_rn(dir.y, den);
-                dz = __fdiv_rn(dir.z, den);
-                px = __int2float_rn(nx);
-                py = __int2float_rn(ny);
-                pz = __int2float_rn(nz);
+                // band end points outside the +-2^23-voxel (+-2^20-block) key range
+                // cannot be stored: flag and skip the pixel (every sample lies
+                // between the two end points)
+                if (!voxel_ok(nx, ny, nz) || !voxel_ok(fx, fy, fz)) {
+                    atomicOr(m.ctr + C_ERR, VMAP_FLAG_RANGE);
+                } else {
+                    float3 dir =
+                        make_float3(__int2float_rn(fx - nx), __int2float_rn(fy - ny), __int2float_rn(fz - nz));
+                    const float len = __fsqrt_rn(sqnorm(dir));
+                    // (int)ceil(2.0 * len): the double product of a float by 2 is exact
+                    n = __float2int_rz(ceilf(__fmul_rn(2.f, len)));
+                    const float den = __int2float_rn(n - 1);
+                    dx = __fdiv_rn(dir.x, den);
+                    dy = __fdiv_rn(dir.y, den);
+                    dz = __fdiv_rn(dir.z, den);
+                    px = __int2float_rn(nx);
+                    py = __int2float_rn(ny);
+                    pz = __int2float_rn(nz);
+                }
             }
         }
     }

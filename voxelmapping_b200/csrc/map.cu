@@ -233,6 +233,10 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
     if ((long long)cfg.num_buckets * kSlots < (long long)cfg.num_entries)
         cfg.num_buckets = (int)(((long long)cfg.num_entries + kSlots - 1) / kSlots);
     if (cfg.truncation == 0) cfg.truncation = cfg.voxel_size * 4;  // vmapping.cpp:59
+    // voxel size >= 0.1 mm keeps ray distances (in voxels, up to 5 m) below 2^24 so
+    // unit steps always advance a float; truncation <= 1024 voxels bounds the
+    // samples per depth pixel
+    if (cfg.voxel_size < 1e-4f || cfg.truncation > 1024.f * cfg.voxel_size) return VMAP_ERR_INVALID_ARG;
     if (cfg.max_weight == 0) cfg.max_weight = 255;                 // depth_fusion.cu:193
     if (cfg.voxel_format == VMAP_VOXEL_REF && cfg.max_weight > 255) return VMAP_ERR_INVALID_ARG;
     if (cfg.max_weight > 65535) return VMAP_ERR_INVALID_ARG;

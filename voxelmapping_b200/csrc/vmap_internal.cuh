@@ -122,6 +122,13 @@ __device__ __forceinline__ bool coord_ok(int x, int y, int z)
            z < kCoordLimit;
 }
 
+// voxel coordinates whose blocks are representable: [-2^23, 2^23)
+__device__ __forceinline__ bool voxel_ok(int x, int y, int z)
+{
+    constexpr int lim = kCoordLimit * kBlockSide;
+    return x >= -lim && x < lim && y >= -lim && y < lim && z >= -lim && z < lim;
+}
+
 __device__ __forceinline__ unsigned long long pack_key(int x, int y, int z)
 {
     return ((unsigned long long)(x & 0x1FFFFF) << 42) | ((unsigned long long)(y & 0x1FFFFF) << 21) |
