@@ -184,6 +184,29 @@ vmap_status vmap_copy_counters(vmap_map* map, uint32_t* dst, void* stream);
 vmap_status vmap_export_blocks(vmap_map* map, int32_t* coords, float* tsdf, float* weight, uint8_t* rgb,
                                uint32_t max_blocks, uint32_t* n_blocks, void* stream);
 
+/* Block export that allocates nothing. No counterpart in the reference.
+ *
+ * Same output as vmap_export_blocks for the blocks [first, first + count) in
+ * pool order: count <= VMAP_EXPORT_STATIC_MAX_BLOCKS; *n_blocks receives how
+ * many exist from `first` on. It is for callers that must not call cudaMalloc
+ * or cudaFree once running: loops under a no-allocation policy, plugins whose
+ * host owns all device memory, code running while a stream is captured into a
+ * CUDA graph. vmap_export_blocks stages through device buffers it allocates on
+ * every call; this entry point stages through one fixed device array of
+ * VMAP_EXPORT_STATIC_MAX_BLOCKS blocks (about 1.4 MiB) that every GPU loading
+ * the library holds until the process exits.
+ *  - count > VMAP_EXPORT_STATIC_MAX_BLOCKS is rejected with
+ *    VMAP_ERR_INVALID_ARG (text in vmap_last_error); loop over `first`.
+ *  - The first call on a device looks up the array's device address; make
+ *    that first call before any stream capture begins.
+ *  - All calls share the one array: calls whose work overlaps on the GPU (other
+ *    threads, streams or maps at the same time) race. Each call overwrites what
+ *    it uses, so nothing needs clearing between calls.
+ *  - Synchronous: returns after the host buffers are filled. */
+#define VMAP_EXPORT_STATIC_MAX_BLOCKS 256
+vmap_status vmap_export_blocks_static(vmap_map* map, uint32_t first, uint32_t count, int32_t* coords, float* tsdf,
+                                      float* weight, uint8_t* rgb, uint32_t* n_blocks, void* stream);
+
 /* ---- stage timing (no counterpart in the reference, which has no timers) --
  * When enabled, every kernel launch of the map is bracketed by CUDA events on
  * the caller's stream; vmap_timing_read synchronises on them and returns the

@@ -79,6 +79,7 @@ SIGNATURES = {
     "vmap_clear_errors": (C.c_int, [P, P]),
     "vmap_export_blocks": (C.c_int, [P, P, P, P, P, C.c_uint32, C.POINTER(C.c_uint32), P]),
     "vmap_copy_counters": (C.c_int, [P, P, P]),
+    "vmap_export_blocks_static": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P, P, P, C.POINTER(C.c_uint32), P]),
     "vmap_timing_enable": (C.c_int, [P, C.c_uint32]),
     "vmap_timing_read": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     "vmap_pose_inverse": (None, [DBL16, DBL16]),

@@ -63,3 +63,11 @@ cudaError_t launch_export(const DevMap& m, int fmt, bool color, int first, int c
                           float* weight, uint8_t* rgb, cudaStream_t s);
 
 }  // namespace vmapb
+
+struct vmap_map;
+#include <string>
+namespace vmapb {
+// map.cu: device view of a map and the text behind vmap_last_error().
+const DevMap& map_device_view(const vmap_map* m);
+void set_last_error(const std::string& msg);
+}  // namespace vmapb
