@@ -230,6 +230,10 @@ vmap_status vmap_timing_read(vmap_map* map, double ms[VMAP_NUM_STAGES], uint32_t
 void vmap_pose_inverse(const double pose[16], double inv[16]);
 /* hash (map_struct.h:104-109), exposed for parity tests. */
 int vmap_block_hash(int x, int y, int z, int n_buckets);
+/* The same hash evaluated on the GPU by the code the hash table uses, for n
+ * block coordinates (xyz_dev: n x 3 int32, device) into out_dev (n int32). */
+vmap_status vmap_block_hash_device(const int32_t* xyz_dev, uint32_t n, int n_buckets, int32_t* out_dev,
+                                   void* stream);
 /* Bytes per voxel block for a format. */
 size_t vmap_block_bytes(int voxel_format, int with_color);
 const char* vmap_status_string(vmap_status s);

@@ -32,8 +32,8 @@ def test_library_exports_every_declared_symbol():
 def test_abi_basics():
     lib = L.lib()
     assert lib.vmap_abi_version() == 1
-    assert lib.vmap_block_bytes(L.VOXEL_REF, 0) == 512 * 3
-    assert lib.vmap_block_bytes(L.VOXEL_REF, 1) == 512 * 6
+    assert lib.vmap_block_bytes(L.VOXEL_REF, 0) == 512 * 4
+    assert lib.vmap_block_bytes(L.VOXEL_REF, 1) == 512 * 7
     assert lib.vmap_block_bytes(L.VOXEL_F32, 1) == 512 * 11
     assert lib.vmap_block_bytes(L.VOXEL_F16, 0) == 512 * 4
     assert lib.vmap_block_bytes(L.VOXEL_I16, 1) == 512 * 7

@@ -84,6 +84,7 @@ SIGNATURES = {
     "vmap_timing_read": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     "vmap_pose_inverse": (None, [DBL16, DBL16]),
     "vmap_block_hash": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
+    "vmap_block_hash_device": (C.c_int, [P, C.c_uint32, C.c_int, P, P]),
     "vmap_block_bytes": (SZ, [C.c_int, C.c_int]),
     "vmap_status_string": (C.c_char_p, [C.c_int]),
     "vmap_last_error": (C.c_char_p, []),

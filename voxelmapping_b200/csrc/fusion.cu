@@ -133,32 +133,31 @@ __global__ void __launch_bounds__(256) visibility_kernel(DevMap m, FrameParams f
 
 // ----------------------------------------------------------------- fusion
 // DepthFusionFunctor / ImageFusionFunctor (depth_fusion.cu:148-196, 328-380).
-// 64 threads per block, one 8-voxel x-row each; 4 blocks per 256-thread CTA,
-// grid-stride over the visible list. A row is read and written (16-byte
-// vector accesses per plane) only when at least one of its voxels updates.
+// 128 threads per block, each owning 4 consecutive voxels of an x-row (one
+// 16- or 32-byte vector of voxel words, one 4-byte word per colour plane);
+// 2 blocks per 256-thread CTA, grid-stride over the visible list. A thread
+// reads and writes its voxels only when at least one of them updates.
 template <int FMT, bool COLOR, int DT>
 __global__ void __launch_bounds__(256) fuse_kernel(DevMap m, FrameParams f)
 {
     typedef Layout<FMT> L;
-    typedef typename L::T T;
-    typedef typename L::W W;
+    typedef typename L::Word Word;
     typedef Fmt<FMT> F;
-    const int team = threadIdx.x >> 6;
-    const int row = threadIdx.x & 63;
-    const int ly = row & 7, lz = row >> 3;
+    const int team = threadIdx.x >> 7;
+    const int v0 = (threadIdx.x & 127) * 4;  // first voxel index of this thread
+    const int lx0 = v0 & 7, ly = (v0 >> 3) & 7, lz = v0 >> 6;
     const int nvis = m.ctr[C_VISIBLE];
-    const int r0 = lz * 64 + ly * 8;
-    for (int i = blockIdx.x * 4 + team; i < nvis; i += gridDim.x * 4) {
+    for (int i = blockIdx.x * 2 + team; i < nvis; i += gridDim.x * 2) {
         const int slot = m.visList[i];
         const int3 bp = unpack_key(m.blockKeys[slot]);
-        const int vx0 = bp.x * 8;
+        const int vx0 = bp.x * 8 + lx0;
         const float wy = __fmul_rn(__int2float_rn(bp.y * 8 + ly), m.vs);
         const float wz = __fmul_rn(__int2float_rn(bp.z * 8 + lz), m.vs);
-        float sdfv[8];
-        int pu[8], pv[8];
+        float sdfv[4];
+        int pu[4], pv[4];
         unsigned mask = 0;
 #pragma unroll
-        for (int x = 0; x < 8; ++x) {
+        for (int x = 0; x < 4; ++x) {
             const float3 p = xf_apply(f.Ti, __fmul_rn(__int2float_rn(vx0 + x), m.vs), wy, wz);
             // __float2int_rd(fx * p0 / p2 + cx + 0.5)
             const int u = __float2int_rd(__fadd_rn(__fadd_rn(__fdiv_rn(__fmul_rn(f.fx, p.x), p.z), f.cx), 0.5f));
@@ -169,39 +168,37 @@ __global__ void __launch_bounds__(256) fuse_kernel(DevMap m, FrameParams f)
             if (u < 0 || v < 0 || u > f.W - 1 || v > f.H - 1) continue;
             const float d = read_depth<DT>(f, u, v);
             if (isnan(d) || d > kMaxDepth || d < kMinDepth) continue;
-            float sdf = __fsub_rn(d, p.z);
+            const float sdf = __fsub_rn(d, p.z);
             if (sdf < -m.mu) continue;
             sdfv[x] = fminf(1.f, __fdiv_rn(sdf, m.mu));
             mask |= 1u << x;
         }
         if (!mask) continue;
-        unsigned char* blk = m.pool + (size_t)slot * m.blockBytes;
-        T t[8];
-        W w[8];
-        load_row<8 * sizeof(T)>(blk + L::kTsdfOff + r0 * sizeof(T), t);
-        load_row<8 * sizeof(W)>(blk + L::kWOff + r0 * sizeof(W), w);
-        unsigned char c[3][8];
+        Word* blk = L::words_rw(m, slot);
+        Word w[4];
+        load_vec<4 * sizeof(Word)>(blk + v0, w);
+        unsigned char c[3][4];
+        unsigned char* crow = reinterpret_cast<unsigned char*>(blk) + L::kRgbOff + v0;
         if constexpr (COLOR) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) load_row<8>(blk + L::kRgbOff + k * kBlockVoxels + r0, c[k]);
+            for (int k = 0; k < 3; ++k) load_vec<4>(crow + k * kBlockVoxels, c[k]);
         }
 #pragma unroll
-        for (int x = 0; x < 8; ++x) {
+        for (int x = 0; x < 4; ++x) {
             if (!(mask & (1u << x))) continue;
-            const float ow = F::wf(w[x]);
+            const float ow = F::weight(w[x]);
             const uint8_t* px = nullptr;
             if constexpr (COLOR) px = f.rgb + (size_t)pv[x] * f.rgbPitch + 3 * pu[x];
             if (ow == 0.f) {
-                t[x] = F::q(sdfv[x]);
-                w[x] = F::wq(1.f);
+                w[x] = F::make(sdfv[x], 1.f);
                 if constexpr (COLOR) {
 #pragma unroll
                     for (int k = 0; k < 3; ++k) c[k][x] = __ldg(px + k);
                 }
             } else {
-                const float os = F::dq(t[x]);
-                t[x] = F::q(__fdiv_rn(__fmaf_rn(os, ow, sdfv[x]), __fadd_rn(ow, 1.f)));
-                w[x] = F::wq(fminf(__fadd_rn(ow, 1.f), m.wmax));
+                const float os = F::tsdf(w[x]);
+                w[x] = F::make(__fdiv_rn(__fmaf_rn(os, ow, sdfv[x]), __fadd_rn(ow, 1.f)),
+                               fminf(__fadd_rn(ow, 1.f), m.wmax));
                 if constexpr (COLOR) {
 #pragma unroll
                     for (int k = 0; k < 3; ++k)
@@ -210,11 +207,10 @@ __global__ void __launch_bounds__(256) fuse_kernel(DevMap m, FrameParams f)
                 }
             }
         }
-        store_row<8 * sizeof(T)>(blk + L::kTsdfOff + r0 * sizeof(T), t);
-        store_row<8 * sizeof(W)>(blk + L::kWOff + r0 * sizeof(W), w);
+        store_vec<4 * sizeof(Word)>(blk + v0, w);
         if constexpr (COLOR) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) store_row<8>(blk + L::kRgbOff + k * kBlockVoxels + r0, c[k]);
+            for (int k = 0; k < 3; ++k) store_vec<4>(crow + k * kBlockVoxels, c[k]);
         }
     }
 }

@@ -182,6 +182,29 @@ int vmap_block_hash(int x, int y, int z, int nb)
     return r < 0 ? r + nb : r;
 }
 
+}  // extern "C"
+
+namespace {
+__global__ void block_hash_kernel(const int* xyz, unsigned n, int nb, unsigned long long magic, int* out)
+{
+    const unsigned i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = ref_hash_fast(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], nb, magic);
+}
+}  // namespace
+
+extern "C" {
+
+vmap_status vmap_block_hash_device(const int32_t* xyz_dev, uint32_t n, int n_buckets, int32_t* out_dev, void* stream)
+{
+    if ((!xyz_dev || !out_dev) && n) return VMAP_ERR_INVALID_ARG;
+    if (n_buckets < 1) return VMAP_ERR_INVALID_ARG;
+    if (n == 0) return VMAP_OK;
+    block_hash_kernel<<<(n + 255) / 256, 256, 0, as_stream(stream)>>>(xyz_dev, n, n_buckets,
+                                                                      bucket_magic((unsigned)n_buckets), out_dev);
+    VMAP_CK(cudaGetLastError());
+    return VMAP_OK;
+}
+
 // Affine inverse of a row-major camera-to-world pose in double:
 // inv(A) = adj(A) / det(A), t' = -inv(A) t (the reference inverts the 4x4 in
 // float with Eigen, depth_fusion.cu:251, ray_tracing.cu:414).
@@ -293,6 +316,7 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
         return st;
     }
     m->dm.nBucket = cfg.num_buckets;
+    m->dm.bucketMagic = bucket_magic((unsigned)cfg.num_buckets);
     m->dm.capacity = cfg.num_blocks;
     m->dm.blockBytes = (int)blockBytes;
     m->dm.vs = cfg.voxel_size;

@@ -72,9 +72,10 @@ __global__ void __launch_bounds__(256) mesh_kernel(DevMap m, float* verts, float
             unsigned char ok = 0;
             if (slot >= 0) {
                 const int li = ((lz & 7) << 6) | ((ly & 7) << 3) | (lx & 7);
-                if (Layout<FMT>::weight(m, slot)[li] != 0) {
+                const typename Fmt<FMT>::Word w = Layout<FMT>::words(m, slot)[li];
+                if (Fmt<FMT>::observed(w)) {
                     ok = 1;
-                    v = Fmt<FMT>::dq(Layout<FMT>::tsdf(m, slot)[li]);
+                    v = Fmt<FMT>::tsdf(w);
                 }
             }
             s_sdf[e] = v;
@@ -197,8 +198,9 @@ __global__ void export_kernel(DevMap m, int first, int count, int* coords, float
         }
         for (int i = threadIdx.x; i < kBlockVoxels; i += blockDim.x) {
             const size_t o = (size_t)b * kBlockVoxels + i;
-            tsdf[o] = Fmt<FMT>::dq(L::tsdf(m, slot)[i]);
-            weight[o] = Fmt<FMT>::wf(L::weight(m, slot)[i]);
+            const typename Fmt<FMT>::Word w = L::words(m, slot)[i];
+            tsdf[o] = Fmt<FMT>::tsdf(w);
+            weight[o] = Fmt<FMT>::weight(w);
             if constexpr (COLOR) {
                 if (rgb) {
                     const unsigned char* c = m.pool + (size_t)slot * m.blockBytes + L::kRgbOff;

@@ -25,44 +25,61 @@
 namespace vmapb {
 
 // ------------------------------------------------------------------ z-range
-// Per allocated block: project the 8 corners, take the pixel bounding box
-// (+1 px) and depth range (+-1 voxel), and fold them into the tile maps with
-// integer atomics (depths are positive, so float order == bit order). A block
-// with a corner at or behind z = 0.05 m covers every tile from depth 0.
+// Per allocated block: the part of the block in front of the plane z = zc
+// (corners in front, plus the points where its 12 edges cross the plane) is
+// projected; its pixel bounding box (+1 px) and depth range (+-1 voxel) are
+// folded into the 8x8-pixel tile maps with integer atomics (depths are
+// positive, so float order == bit order). Every point of a block is a convex
+// combination of its corners, so the box and range bound every ray sample
+// that can fall inside the block.
+constexpr float kClipZ = 0.05f;  // below the ray start depth of 0.1 m
+
 __global__ void __launch_bounds__(256) zrange_kernel(DevMap m, RenderParams r)
 {
     const int n = allocated_blocks(m);
     const float scale = m.vs * 8.f;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int3 b = unpack_key(m.blockKeys[i]);
-        float zlo = 1e30f, zhi = -1e30f, umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
-        bool near = false;
+        float3 p[8];
+        float zlo = 1e30f, zhi = -1e30f;
 #pragma unroll
         for (int c = 0; c < 8; ++c) {
-            const float3 p = xf_apply(r.Ti, (float)(b.x + (c & 1)) * scale, (float)(b.y + ((c >> 1) & 1)) * scale,
-                                      (float)(b.z + ((c >> 2) & 1)) * scale);
-            zlo = fminf(zlo, p.z);
-            zhi = fmaxf(zhi, p.z);
-            if (p.z <= 0.05f) {
-                near = true;
-                continue;
-            }
-            const float u = r.fx * p.x / p.z + r.cx, v = r.fy * p.y / p.z + r.cy;
+            p[c] = xf_apply(r.Ti, (float)(b.x + (c & 1)) * scale, (float)(b.y + ((c >> 1) & 1)) * scale,
+                            (float)(b.z + ((c >> 2) & 1)) * scale);
+            zlo = fminf(zlo, p[c].z);
+            zhi = fmaxf(zhi, p[c].z);
+        }
+        if (zhi <= kClipZ || zhi < kMinDepth - m.vs || zlo > kMaxDepth + m.vs) continue;
+        float umin = 1e30f, umax = -1e30f, vmin = 1e30f, vmax = -1e30f;
+        auto add = [&](float3 q) {
+            const float iz = 1.f / q.z;
+            const float u = r.fx * q.x * iz + r.cx, v = r.fy * q.y * iz + r.cy;
             umin = fminf(umin, u);
             umax = fmaxf(umax, u);
             vmin = fminf(vmin, v);
             vmax = fmaxf(vmax, v);
+        };
+#pragma unroll
+        for (int c = 0; c < 8; ++c)
+            if (p[c].z > kClipZ) add(p[c]);
+        if (zlo <= kClipZ) {  // the block crosses the clip plane: add the edge crossings
+#pragma unroll
+            for (int c = 0; c < 8; ++c)
+#pragma unroll
+                for (int bit = 1; bit < 8; bit <<= 1) {
+                    if (c & bit) continue;
+                    const float3 a = p[c], e = p[c | bit];
+                    if ((a.z > kClipZ) == (e.z > kClipZ)) continue;
+                    const float t = (kClipZ - a.z) / (e.z - a.z);
+                    add(make_float3(a.x + t * (e.x - a.x), a.y + t * (e.y - a.y), kClipZ));
+                }
         }
-        if (zhi < kMinDepth - m.vs || zlo > kMaxDepth + m.vs) continue;
-        int tx0 = 0, tx1 = r.tilesX - 1, ty0 = 0, ty1 = r.tilesY - 1;
-        if (!near) {
-            if (umax < -1.f || vmax < -1.f || umin > (float)r.W || vmin > (float)r.H) continue;
-            tx0 = max(0, (int)floorf(umin - 1.f) >> 3);
-            tx1 = min(r.tilesX - 1, (int)floorf(umax + 1.f) >> 3);
-            ty0 = max(0, (int)floorf(vmin - 1.f) >> 3);
-            ty1 = min(r.tilesY - 1, (int)floorf(vmax + 1.f) >> 3);
-        }
-        const unsigned lo = __float_as_uint(near ? 0.f : fmaxf(zlo - m.vs, 0.f));
+        if (umax < -1.f || vmax < -1.f || umin > (float)r.W || vmin > (float)r.H) continue;
+        const int tx0 = max(0, (int)floorf(fmaxf(umin - 1.f, -8.f)) >> 3);
+        const int tx1 = min(r.tilesX - 1, (int)floorf(fminf(umax + 1.f, (float)r.W + 8.f)) >> 3);
+        const int ty0 = max(0, (int)floorf(fmaxf(vmin - 1.f, -8.f)) >> 3);
+        const int ty1 = min(r.tilesY - 1, (int)floorf(fminf(vmax + 1.f, (float)r.H + 8.f)) >> 3);
+        const unsigned lo = __float_as_uint(fmaxf(zlo - m.vs, 0.f));
         const unsigned hi = __float_as_uint(zhi + m.vs);
         for (int ty = ty0; ty <= ty1; ++ty)
             for (int tx = tx0; tx <= tx1; ++tx) {
@@ -99,11 +116,10 @@ struct RayCtx {
     __device__ __forceinline__ float voxel(int slot, int vx, int vy, int vz, bool& valid) const
     {
         if (slot >= 0) {
-            const int li = local_idx(vx, vy, vz);
-            const typename Fmt<FMT>::W w = __ldg(Layout<FMT>::weight(m, slot) + li);
-            if (w != 0) {
+            const typename Fmt<FMT>::Word w = __ldg(Layout<FMT>::words(m, slot) + local_idx(vx, vy, vz));
+            if (Fmt<FMT>::observed(w)) {
                 valid = true;
-                return Fmt<FMT>::dq(__ldg(Layout<FMT>::tsdf(m, slot) + li));
+                return Fmt<FMT>::tsdf(w);
             }
         }
         valid = false;
@@ -177,6 +193,10 @@ __global__ void __launch_bounds__(256) raycast_kernel(DevMap m, RenderParams r, 
     float3 be = xf_apply(r.T, p1.x, p1.y, p1.z);
     be = make_float3(__fmul_rn(be.x, r.vsinv), __fmul_rn(be.y, r.vsinv), __fmul_rn(be.z, r.vsinv));
     const float3 dir = normalized(make_float3(__fsub_rn(be.x, bs.x), __fsub_rn(be.y, bs.y), __fsub_rn(be.z, bs.z)));
+    // exit faces: +8 along axes the ray runs up (and +0), +0 along axes it runs
+    // down (and -0), so a zero component gives an infinite exit distance
+    const float3 inv = make_float3(__frcp_rn(dir.x), __frcp_rn(dir.y), __frcp_rn(dir.z));
+    const int ox = signbit(dir.x) ? 0 : 8, oy = signbit(dir.y) ? 0 : 8, oz = signbit(dir.z) ? 0 : 8;
 
     float3 res = bs;
     float dist_s = dist0;
@@ -209,13 +229,12 @@ __global__ void __launch_bounds__(256) raycast_kernel(DevMap m, RenderParams r, 
         if (ctx.cblk < 0) {
             // every 1-voxel step inside this unallocated block reads (1.0, invalid):
             // jump to the last step that is still inside (at least one step)
-            float t = 1e30f;
-            if (dir.x > 0.f) t = fminf(t, ((float)(bx * 8 + 8) - res.x) / dir.x);
-            else if (dir.x < 0.f) t = fminf(t, ((float)(bx * 8) - res.x) / dir.x);
-            if (dir.y > 0.f) t = fminf(t, ((float)(by * 8 + 8) - res.y) / dir.y);
-            else if (dir.y < 0.f) t = fminf(t, ((float)(by * 8) - res.y) / dir.y);
-            if (dir.z > 0.f) t = fminf(t, ((float)(bz * 8 + 8) - res.z) / dir.z);
-            else if (dir.z < 0.f) t = fminf(t, ((float)(bz * 8) - res.z) / dir.z);
+            // distance to the block's exit face along each axis (the far face
+            // is the one the direction points at; inv is +-inf on a zero axis)
+            const float tx = ((float)(bx * 8 + ox) - res.x) * inv.x;
+            const float ty = ((float)(by * 8 + oy) - res.y) * inv.y;
+            const float tz = ((float)(bz * 8 + oz) - res.z) * inv.z;
+            const float t = fminf(fminf(tx, ty), tz);  // fminf drops the NaN of 0 * inf
             const float k = fmaxf(1.f, ceilf(t - 1e-3f));
             res = fma3(k, dir, res);
             dist_s = __fadd_rn(dist_s, k);

@@ -54,6 +54,7 @@ struct DevMap {
     unsigned char* pool;           // capacity * blockBytes
     unsigned* ctr;                 // C_COUNT counters
     int* visList;                  // capacity: visible block slots
+    unsigned long long bucketMagic;  // ceil(2^64 / nBucket): remainder by multiplication
     int nBucket;
     int capacity;
     int blockBytes;
@@ -150,6 +151,23 @@ __device__ __forceinline__ int ref_hash(int x, int y, int z, int nb)
     return r < 0 ? r + nb : r;
 }
 
+// The same value with the remainder taken by multiplication (Lemire, Kaser and
+// Kurz, "Faster remainder by direct computation", 2019): for 32-bit a and d,
+// a mod d = hi64((M * a mod 2^64) * d) with M = ceil(2^64 / d). C's remainder
+// of a negative r has the sign of r, so |r| mod d is negated and shifted.
+__host__ __device__ __forceinline__ unsigned long long bucket_magic(unsigned d)
+{
+    return ~0ull / d + 1ull;
+}
+
+__device__ __forceinline__ int ref_hash_fast(int x, int y, int z, int nb, unsigned long long magic)
+{
+    const int r = (int)(((unsigned)x * 73856093u) ^ ((unsigned)y * 19349669u) ^ ((unsigned)z * 83492791u));
+    const unsigned a = r < 0 ? 0u - (unsigned)r : (unsigned)r;
+    const unsigned mod = (unsigned)__umul64hi(magic * a, (unsigned long long)nb);
+    return r < 0 ? (mod ? nb - (int)mod : 0) : (int)mod;
+}
+
 // checkBlockVisible (map_struct.h:219-244): any of the 8 block corners
 // projects inside [0, cols-1] x [0, rows-1] with depth in [0.1, 5].
 __device__ __forceinline__ bool block_visible(int bx, int by, int bz, const Xf& ti, float scale, int cols,
@@ -178,7 +196,7 @@ __device__ __forceinline__ int hash_find(const DevMap& m, int bx, int by, int bz
 {
     if (!coord_ok(bx, by, bz)) return -1;
     const unsigned long long key = pack_key(bx, by, bz);
-    int b = ref_hash(bx, by, bz, m.nBucket);
+    int b = ref_hash_fast(bx, by, bz, m.nBucket, m.bucketMagic);
 #pragma unroll 1
     for (int p = 0; p < kMaxProbe; ++p) {
         const ulonglong2* s = reinterpret_cast<const ulonglong2*>(m.keys + (size_t)b * kSlots);
@@ -204,7 +222,7 @@ __device__ __forceinline__ int hash_find(const DevMap& m, int bx, int by, int bz
 __device__ __forceinline__ void hash_insert(const DevMap& m, int bx, int by, int bz)
 {
     const unsigned long long key = pack_key(bx, by, bz);
-    int b = ref_hash(bx, by, bz, m.nBucket);
+    int b = ref_hash_fast(bx, by, bz, m.nBucket, m.bucketMagic);
 #pragma unroll 1
     for (int p = 0; p < kMaxProbe; ++p) {
         unsigned long long* s = m.keys + (size_t)b * kSlots;
@@ -243,79 +261,87 @@ __device__ __forceinline__ int allocated_blocks(const DevMap& m)
 }
 
 // ------------------------------------------------------------ voxel formats
-// Per-block plane layout: [tsdf x512][weight x512][r x512][g x512][b x512].
+// Each voxel's TSDF and weight share one word so a sample is one load:
+// 4 bytes (REF, F16, I16) or 8 bytes (F32). Block layout in the pool:
+// [word x512][r x512][g x512][b x512], voxel index x + 8y + 64z; colour
+// planes only when the map keeps colour. A voxel with weight 0 is unobserved.
 template <int FMT>
 struct Fmt;
 
 template <>
-struct Fmt<VMAP_VOXEL_REF> {  // reference Voxel: int16 x32767, uint8 weight
-    typedef short T;
-    typedef unsigned char W;
+struct Fmt<VMAP_VOXEL_REF> {  // reference Voxel: int16 x32767 tsdf, uint8 weight
+    typedef unsigned Word;      // bits 0-15 tsdf code, 16-23 weight
     // unpackFloat (map_struct.h:72-75): val / 32767.f
-    static __device__ __forceinline__ float dq(T c) { return __fdiv_rn(__int2float_rn(c), 32767.f); }
+    static __device__ __forceinline__ float tsdf(Word w) { return __fdiv_rn(__int2float_rn((short)(w & 0xffffu)), 32767.f); }
+    static __device__ __forceinline__ float weight(Word w) { return __uint2float_rn((w >> 16) & 0xffu); }
+    static __device__ __forceinline__ bool observed(Word w) { return (w >> 16) != 0u; }
     // packFloat (map_struct.h:77-80): (short)(val * 32767), truncation
-    static __device__ __forceinline__ T q(float v) { return (short)__float2int_rz(__fmul_rn(v, 32767.f)); }
-    static __device__ __forceinline__ float wf(W w) { return (float)w; }
-    static __device__ __forceinline__ W wq(float w) { return (W)__float2uint_rz(w); }
+    static __device__ __forceinline__ Word make(float t, float wt)
+    {
+        return (unsigned)(unsigned short)(short)__float2int_rz(__fmul_rn(t, 32767.f)) | (__float2uint_rz(wt) << 16);
+    }
 };
 
 template <>
 struct Fmt<VMAP_VOXEL_F32> {
-    typedef float T;
-    typedef float W;
-    static __device__ __forceinline__ float dq(T c) { return c; }
-    static __device__ __forceinline__ T q(float v) { return v; }
-    static __device__ __forceinline__ float wf(W w) { return w; }
-    static __device__ __forceinline__ W wq(float w) { return w; }
+    typedef float2 Word;  // x tsdf, y weight
+    static __device__ __forceinline__ float tsdf(Word w) { return w.x; }
+    static __device__ __forceinline__ float weight(Word w) { return w.y; }
+    static __device__ __forceinline__ bool observed(Word w) { return w.y != 0.f; }
+    static __device__ __forceinline__ Word make(float t, float wt) { return make_float2(t, wt); }
 };
 
 template <>
 struct Fmt<VMAP_VOXEL_F16> {
-    typedef unsigned short T;  // IEEE half bits
-    typedef unsigned short W;
-    static __device__ __forceinline__ float dq(T c) { return __half2float(__ushort_as_half(c)); }
-    static __device__ __forceinline__ T q(float v) { return __half_as_ushort(__float2half_rn(v)); }
-    static __device__ __forceinline__ float wf(W w) { return (float)w; }
-    static __device__ __forceinline__ W wq(float w) { return (W)__float2uint_rz(w); }
+    typedef unsigned Word;  // bits 0-15 IEEE half tsdf, 16-31 uint16 weight
+    static __device__ __forceinline__ float tsdf(Word w) { return __half2float(__ushort_as_half((unsigned short)(w & 0xffffu))); }
+    static __device__ __forceinline__ float weight(Word w) { return __uint2float_rn(w >> 16); }
+    static __device__ __forceinline__ bool observed(Word w) { return (w >> 16) != 0u; }
+    static __device__ __forceinline__ Word make(float t, float wt)
+    {
+        return (unsigned)__half_as_ushort(__float2half_rn(t)) | (__float2uint_rz(wt) << 16);
+    }
 };
 
 template <>
 struct Fmt<VMAP_VOXEL_I16> {
-    typedef short T;
-    typedef unsigned short W;
-    static __device__ __forceinline__ float dq(T c) { return __fdiv_rn(__int2float_rn(c), 32767.f); }
-    static __device__ __forceinline__ T q(float v) { return (short)__float2int_rz(__fmul_rn(v, 32767.f)); }
-    static __device__ __forceinline__ float wf(W w) { return (float)w; }
-    static __device__ __forceinline__ W wq(float w) { return (W)__float2uint_rz(w); }
+    typedef unsigned Word;  // bits 0-15 int16 x32767 tsdf, 16-31 uint16 weight
+    static __device__ __forceinline__ float tsdf(Word w) { return __fdiv_rn(__int2float_rn((short)(w & 0xffffu)), 32767.f); }
+    static __device__ __forceinline__ float weight(Word w) { return __uint2float_rn(w >> 16); }
+    static __device__ __forceinline__ bool observed(Word w) { return (w >> 16) != 0u; }
+    static __device__ __forceinline__ Word make(float t, float wt)
+    {
+        return (unsigned)(unsigned short)(short)__float2int_rz(__fmul_rn(t, 32767.f)) | (__float2uint_rz(wt) << 16);
+    }
 };
 
 template <int FMT>
 struct Layout {
-    typedef typename Fmt<FMT>::T T;
-    typedef typename Fmt<FMT>::W W;
-    static constexpr int kTsdfOff = 0;
-    static constexpr int kWOff = kBlockVoxels * (int)sizeof(T);
-    static constexpr int kRgbOff = kBlockVoxels * (int)(sizeof(T) + sizeof(W));
+    typedef typename Fmt<FMT>::Word Word;
+    static constexpr int kWordBytes = (int)sizeof(Word);
+    static constexpr int kRgbOff = kBlockVoxels * kWordBytes;
     static __host__ __device__ constexpr int bytes(bool color)
     {
-        return kBlockVoxels * (int)(sizeof(T) + sizeof(W)) + (color ? 3 * kBlockVoxels : 0);
+        return kBlockVoxels * kWordBytes + (color ? 3 * kBlockVoxels : 0);
     }
-    static __device__ __forceinline__ const T* tsdf(const DevMap& m, int slot)
+    static __device__ __forceinline__ const Word* words(const DevMap& m, int slot)
     {
-        return reinterpret_cast<const T*>(m.pool + (size_t)slot * m.blockBytes + kTsdfOff);
+        return reinterpret_cast<const Word*>(m.pool + (size_t)slot * m.blockBytes);
     }
-    static __device__ __forceinline__ const W* weight(const DevMap& m, int slot)
+    static __device__ __forceinline__ Word* words_rw(const DevMap& m, int slot)
     {
-        return reinterpret_cast<const W*>(m.pool + (size_t)slot * m.blockBytes + kWOff);
+        return reinterpret_cast<Word*>(m.pool + (size_t)slot * m.blockBytes);
     }
 };
 
-// 16-byte vectorised copies of a row of 8 voxels.
+// 16-byte vectorised copies of NBYTES (a multiple of 4; 16-byte aligned when >= 16).
 template <int NBYTES>
-__device__ __forceinline__ void load_row(const void* src, void* dst)
+__device__ __forceinline__ void load_vec(const void* src, void* dst)
 {
-    static_assert(NBYTES == 8 || NBYTES % 16 == 0, "row size");
-    if constexpr (NBYTES == 8) {
+    static_assert(NBYTES == 4 || NBYTES == 8 || NBYTES % 16 == 0, "vector size");
+    if constexpr (NBYTES == 4) {
+        *reinterpret_cast<unsigned*>(dst) = *reinterpret_cast<const unsigned*>(src);
+    } else if constexpr (NBYTES == 8) {
         *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
     } else {
 #pragma unroll
@@ -325,9 +351,11 @@ __device__ __forceinline__ void load_row(const void* src, void* dst)
 }
 
 template <int NBYTES>
-__device__ __forceinline__ void store_row(void* dst, const void* src)
+__device__ __forceinline__ void store_vec(void* dst, const void* src)
 {
-    if constexpr (NBYTES == 8) {
+    if constexpr (NBYTES == 4) {
+        *reinterpret_cast<unsigned*>(dst) = *reinterpret_cast<const unsigned*>(src);
+    } else if constexpr (NBYTES == 8) {
         *reinterpret_cast<uint2*>(dst) = *reinterpret_cast<const uint2*>(src);
     } else {
 #pragma unroll
