@@ -44,6 +44,9 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--num-blocks", type=int, default=0, help="override the block pool (small profiling runs)")
+    p.add_argument("--batch", type=int, default=32, help="maps per batched step (0 skips the batched arm)")
+    p.add_argument("--batch-steps", type=int, default=0, help="timed batched steps (default: --steps // 4)")
+    p.add_argument("--batch-blocks", type=int, default=1 << 17, help="block pool per batched map")
     return p.parse_args()
 
 
@@ -175,6 +178,95 @@ def run_reference(args):
                                        % (args.warmup, args.warmup + args.steps - 1, WORKLOAD)},
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+# -------------------------------------------------------------- batched arm
+def run_batched(args, wl, dev, flush, world, plain_value):
+    """B maps of the same 640x480 / 5 mm workload, FP16 TSDF + uint16 weight +
+    colour, each fed its own seeded scene; one vmap_batch_step per step (one
+    launch per stage over all maps, graph-replayed on a side stream)."""
+    import dataclasses
+
+    import torch
+    import torch.distributed as dist
+    from voxelmapping_b200 import MapBatch, VoxelMapping
+    from voxelmapping_b200 import _lib as L
+    from voxelmapping_b200 import synth
+
+    rank = int(os.environ.get("RANK", 0))
+    B = args.batch
+    K = args.batch_steps or max(4, args.steps // 4)
+    W = min(args.warmup, 5)
+    nfr = W + K
+    wlb = dataclasses.replace(wl, voxel_format="f16", max_weight=128, num_blocks=args.batch_blocks)
+    H, Wd = wlb.height, wlb.width
+    depth = torch.empty((B, nfr, H, Wd), dtype=torch.int16, device=dev)
+    rgb = torch.empty((B, nfr, H, Wd * 3), dtype=torch.uint8, device=dev)
+    poses = np.zeros((B, nfr, 16))
+    for b in range(B):
+        sc = synth.Scene(dataclasses.replace(wlb, seed=1000 * (rank + 1) + b))
+        for i in range(nfr):
+            d, c, p = sc.render(i)
+            depth[b, i].copy_(torch.from_numpy(d.view(np.int16)))
+            rgb[b, i].copy_(torch.from_numpy(c).reshape(H, Wd * 3))
+            poses[b, i] = p.reshape(16)
+        del sc
+    maps = []
+    for b in range(B):
+        vm = VoxelMapping(Wd, H, wlb.K, voxel_format="f16", with_color=True, max_weight=128)
+        vm.CreateMap(wlb.num_entries, wlb.num_blocks, wlb.voxel_size)
+        maps.append(vm)
+    batch = MapBatch(maps)
+    vmaps = torch.empty((B, H, Wd, 4), dtype=torch.float32, device=dev)
+    nmaps = torch.empty_like(vmaps)
+    frames = []
+    for i in range(nfr):
+        fr = (L.BatchFrame * B)()
+        for b in range(B):
+            f = fr[b]
+            f.depth_dev, f.depth_type, f.depth_pitch, f.depth_scale = depth[b, i].data_ptr(), L.DEPTH_U16, Wd * 2, \
+                wlb.depth_scale
+            f.rgb_dev, f.rgb_pitch = rgb[b, i].data_ptr(), Wd * 3
+            for k in range(16):
+                f.pose[k] = poses[b, i, k]
+            f.vmap_dev, f.vmap_pitch = vmaps[b].data_ptr(), Wd * 16
+            f.nmap_dev, f.nmap_pitch = nmaps[b].data_ptr(), Wd * 16
+        frames.append(fr)
+    lib = L.lib()
+    side = torch.cuda.Stream(device=dev)
+    sp = C.c_void_p(side.cuda_stream)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        for i in range(W):
+            L.check(lib.vmap_batch_step(batch._h, frames[i], sp))
+        side.synchronize()
+        if world > 1:
+            dist.barrier()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+        for k in range(K):
+            flush.fill_(k & 255)
+            ev[k][0].record(side)
+            L.check(lib.vmap_batch_step(batch._h, frames[W + k], sp))
+            ev[k][1].record(side)
+        side.synchronize()
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    value = world * B * K / (float(t.item()) / 1e3)
+    hits = float(torch.isfinite(vmaps[:, :, :, 0]).float().mean().item())
+    flags = [m.stats()["error_flags"] for m in maps]
+    batch.release()
+    for m in maps:
+        m.release()
+    return {"value": value, "unit": "frames/s", "maps": B, "steps": K, "warmup": W,
+            "ms_per_step": float(t.item()) / K, "p50_ms_per_step": percentile(step_ms, 50),
+            "p99_ms_per_step": percentile(step_ms, 99), "ratio_vs_plain": value / plain_value,
+            "dtype": "f16", "hit_fraction_last_step": hits, "error_flags": int(max(flags)),
+            "config": "%d maps x 640x480 depth + rgb, 5 mm voxels, FP16 TSDF + uint16 weight (cap 128) + uint8x3 "
+                      "colour, 2^%d-block pool each, each map its own seeded room scene and figure-8; one step = "
+                      "one frame per map fused + raycast (vmap_batch_step: one launch per stage over all maps, "
+                      "CUDA-graph replay); L2 flushed between steps" % (B, int(np.log2(wlb.num_blocks)))}
 
 
 # --------------------------------------------------------------- product arm
@@ -332,6 +424,11 @@ def run_product(args):
                        "h2d_bytes_per_step": P * 2 + P * 3, "d2h_bytes_per_step": 2 * P * 16,
                        "p50_ms": percentile(e_ms, 50), "p99_ms": percentile(e_ms, 99),
                        "path": "vmap_fuse_host + vmap_render_scene_host, pinned host buffers"}
+
+    # --- batched arm: many maps per step ------------------------------------
+    if args.batch > 0:
+        vm.release()
+        line["batched"] = run_batched(args, wl, dev, flush, world, value)
 
     # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

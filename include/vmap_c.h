@@ -168,6 +168,38 @@ vmap_status vmap_polygonize_host(vmap_map* map, const float** verts, const float
  * centroids, 3 floats each. */
 vmap_status vmap_surface_points(const float* verts_dev, uint32_t n_tris, float* points_dev, void* stream);
 
+/* ---- batches (no counterpart in the reference, which drives one map per call)
+ * A batch fuses and raycasts many independent maps per step: frame i goes into
+ * maps[i], which is then raycast at the same pose. Every stage is one launch
+ * covering all maps; the ray marcher is one persistent launch draining a
+ * device-side queue of pixel tiles from every map. On a non-default stream the
+ * first two steps record the step as CUDA graphs that later steps replay (the
+ * per-map descriptors are refreshed by one pinned-memory copy per step).
+ * Maps keep their own sizes, cameras, voxel sizes and pools; all maps of a
+ * batch share one voxel format. A map may belong to several batches but only
+ * one step may use it at a time. */
+typedef struct vmap_batch vmap_batch;
+typedef struct vmap_batch_frame {
+    const void* depth_dev;   /* map-sized depth image                        */
+    int depth_type;          /* vmap_depth_type                              */
+    size_t depth_pitch;      /* bytes, 0 = packed                            */
+    float depth_scale;       /* uint16 -> metres                             */
+    const uint8_t* rgb_dev;  /* uint8x3 or NULL (no colour this step)        */
+    size_t rgb_pitch;
+    double pose[16];         /* camera-to-world, row-major                   */
+    float* vmap_dev;         /* float4 vertex map out, 16-byte aligned       */
+    size_t vmap_pitch;
+    float* nmap_dev;         /* float4 normal map out or NULL                */
+    size_t nmap_pitch;
+} vmap_batch_frame;
+
+#define VMAP_MAX_BATCH 256
+vmap_status vmap_batch_create(vmap_map* const* maps, int n_maps, vmap_batch** out);
+vmap_status vmap_batch_destroy(vmap_batch* batch);
+/* frames: n_maps entries. Asynchronous on `stream`; may block only until the
+ * step before last has copied its descriptors. */
+vmap_status vmap_batch_step(vmap_batch* batch, const vmap_batch_frame* frames, void* stream);
+
 /* ---- inspection ---------------------------------------------------------- */
 /* Synchronises `stream`, then reads the device counters. */
 vmap_status vmap_get_stats(vmap_map* map, void* stream, vmap_stats* out);

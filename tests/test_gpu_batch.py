@@ -1,0 +1,88 @@
+"""Batched fuse + raycast (vmap_batch_*): a batch step over maps of different
+image sizes, cameras, voxel sizes and pools must leave every map, vertex map
+and normal map bit-identical to driving each map on its own. Steps run on a
+side stream so the graph recording (steps 1-2) and replay (steps 3+) are both
+covered."""
+import dataclasses
+
+import numpy as np
+import pytest
+import torch
+
+from tests.common import block_keys
+from voxelmapping_b200 import MapBatch, VoxelMapping
+from voxelmapping_b200 import _lib as L
+from voxelmapping_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def workloads():
+    small = synth.WORKLOADS["room_small"]
+    full = synth.WORKLOADS["room_full"]
+    return [
+        dataclasses.replace(small, seed=11, voxel_format="f16", num_blocks=1 << 16, with_color=True),
+        dataclasses.replace(small, name="ragged", width=203, height=117, fx=181.3, fy=179.9, cx=97.2, cy=55.7,
+                            seed=12, voxel_format="f16", voxel_size=0.012, num_blocks=1 << 14, with_color=False,
+                            room=(2.5, 3.0, 2.5), cam_radius=0.6, cam_height=1.2),
+        dataclasses.replace(full, seed=13, voxel_format="f16", num_blocks=1 << 16, with_color=True),
+    ]
+
+
+def make_map(wl):
+    vm = VoxelMapping(wl.width, wl.height, wl.K, voxel_format=wl.voxel_format, with_color=wl.with_color,
+                      max_weight=128)
+    vm.CreateMap(1 << 18, wl.num_blocks, wl.voxel_size)
+    return vm
+
+
+def test_batch_step_equals_single_map_calls():
+    wls = workloads()
+    scenes = [synth.Scene(wl) for wl in wls]
+    batch_maps = [make_map(wl) for wl in wls]
+    solo_maps = [make_map(wl) for wl in wls]
+    batch = MapBatch(batch_maps)
+    side = torch.cuda.Stream()
+    for step in range(5):
+        depths, rgbs, poses, vb, nb = [], [], [], [], []
+        for wl, sc in zip(wls, scenes):
+            d, c, p = sc.render(step * 3)
+            depths.append(torch.from_numpy(d.view(np.int16)).cuda())
+            rgbs.append(torch.from_numpy(c).cuda().reshape(wl.height, -1) if wl.with_color else None)
+            poses.append(p)
+            vb.append(torch.full((wl.height, wl.width, 4), 7.0, device="cuda"))
+            nb.append(torch.full((wl.height, wl.width, 4), 7.0, device="cuda"))
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            batch.step(depths, rgbs, poses, vb, nb)
+        side.synchronize()
+        for i, (wl, vm) in enumerate(zip(wls, solo_maps)):
+            if wl.with_color:
+                vm.FuseDepthAndImage(rgbs[i], depths[i], poses[i])
+            else:
+                vm.FuseDepth(depths[i], poses[i])
+            nm = torch.empty_like(vb[i])
+            v = vm.RenderScene(None, poses[i], nmap=nm)
+            torch.cuda.synchronize()
+            assert np.array_equal(np.nan_to_num(v.cpu().numpy(), nan=-9.0), np.nan_to_num(vb[i].cpu().numpy(), nan=-9.0)), (step, i)
+            assert np.array_equal(np.nan_to_num(nm.cpu().numpy(), nan=-9.0), np.nan_to_num(nb[i].cpu().numpy(), nan=-9.0)), (step, i)
+            assert np.isfinite(v.cpu().numpy()[..., 0]).mean() > 0.3
+    for wl, a, b in zip(wls, batch_maps, solo_maps):
+        ea, eb = a.export_blocks(), b.export_blocks()
+        ia, ib = np.argsort(block_keys(ea["coords"])), np.argsort(block_keys(eb["coords"]))
+        for k in ("coords", "tsdf", "weight") + (("rgb",) if wl.with_color else ()):
+            assert np.array_equal(ea[k][ia], eb[k][ib]), k
+        assert a.stats()["error_flags"] == 0
+    batch.release()
+
+
+def test_batch_rejects_mixed_formats_and_duplicates():
+    wl = synth.WORKLOADS["room_small"]
+    a = VoxelMapping(wl.width, wl.height, wl.K, voxel_format="f16", with_color=False)
+    a.CreateMap(1 << 14, 1 << 12, wl.voxel_size)
+    b = VoxelMapping(wl.width, wl.height, wl.K, voxel_format="f32", with_color=False)
+    b.CreateMap(1 << 14, 1 << 12, wl.voxel_size)
+    with pytest.raises(L.VmapError):
+        MapBatch([a, b])
+    with pytest.raises(L.VmapError):
+        MapBatch([a, a])

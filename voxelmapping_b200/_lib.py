@@ -53,6 +53,13 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class BatchFrame(C.Structure):
+    _fields_ = [("depth_dev", C.c_void_p), ("depth_type", C.c_int), ("depth_pitch", C.c_size_t),
+                ("depth_scale", C.c_float), ("rgb_dev", C.c_void_p), ("rgb_pitch", C.c_size_t),
+                ("pose", C.c_double * 16), ("vmap_dev", C.c_void_p), ("vmap_pitch", C.c_size_t),
+                ("nmap_dev", C.c_void_p), ("nmap_pitch", C.c_size_t)]
+
+
 P = C.c_void_p
 SZ = C.c_size_t
 DBL16 = C.POINTER(C.c_double)
@@ -75,6 +82,9 @@ SIGNATURES = {
     "vmap_polygonize_host": (C.c_int, [P, C.POINTER(C.POINTER(C.c_float)), C.POINTER(C.POINTER(C.c_float)),
                                        C.POINTER(C.c_uint32), P]),
     "vmap_surface_points": (C.c_int, [P, C.c_uint32, P, P]),
+    "vmap_batch_create": (C.c_int, [C.POINTER(P), C.c_int, C.POINTER(P)]),
+    "vmap_batch_destroy": (C.c_int, [P]),
+    "vmap_batch_step": (C.c_int, [P, C.POINTER(BatchFrame), P]),
     "vmap_get_stats": (C.c_int, [P, P, C.POINTER(Stats)]),
     "vmap_clear_errors": (C.c_int, [P, P]),
     "vmap_export_blocks": (C.c_int, [P, P, P, P, P, C.c_uint32, C.POINTER(C.c_uint32), P]),

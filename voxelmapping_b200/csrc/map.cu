@@ -22,8 +22,9 @@ struct vmap_map {
     size_t poolBytes;
     size_t deviceBytes;
     unsigned* hCtr;           // pinned readback of the counters
-    unsigned* zmin;           // z-range tiles
-    unsigned* zmax;
+    unsigned long long* zmin; // z-range tiles (epoch-tagged)
+    unsigned long long* zmax;
+    unsigned epoch;           // render epoch of the tiles
     int tilesX, tilesY;
     void* dDepth;             // staging for host-buffer calls
     uint8_t* dRgb;
@@ -73,27 +74,56 @@ bool pose_ok(const double p[16])
     return true;
 }
 
-void make_frame(const vmap_map* m, const double pose[16], FrameParams& f)
+}  // namespace
+
+namespace vmapb {
+// The per-step view of a map: storage, camera, pose (FP64 inverse rounded to
+// FP32), no frame inputs and no render outputs yet.
+void make_view(const vmap_map* m, const double pose[16], MapView& v)
 {
-    f.W = m->cfg.width;
-    f.H = m->cfg.height;
-    f.fx = m->cfg.fx;
-    f.fy = m->cfg.fy;
-    f.cx = m->cfg.cx;
-    f.cy = m->cfg.cy;
-    f.ifx = (float)(1.0 / (double)m->cfg.fx);
-    f.ify = (float)(1.0 / (double)m->cfg.fy);
-    double inv[16];
-    vmap_pose_inverse(pose, inv);
-    to_xf(pose, f.T);
-    to_xf(inv, f.Ti);
-    f.depth = nullptr;
-    f.dpitch = 0;
-    f.dtype = 0;
-    f.dscale = 1.f;
-    f.rgb = nullptr;
-    f.rgbPitch = 0;
+    std::memset(&v, 0, sizeof(v));
+    v.m = m->dm;
+    v.cam.W = m->cfg.width;
+    v.cam.H = m->cfg.height;
+    v.cam.fx = m->cfg.fx;
+    v.cam.fy = m->cfg.fy;
+    v.cam.cx = m->cfg.cx;
+    v.cam.cy = m->cfg.cy;
+    v.cam.ifx = (float)(1.0 / (double)m->cfg.fx);
+    v.cam.ify = (float)(1.0 / (double)m->cfg.fy);
+    v.in.dscale = 1.f;
+    if (pose) {
+        double inv[16];
+        vmap_pose_inverse(pose, inv);
+        to_xf(pose, v.T);
+        to_xf(inv, v.Ti);
+    }
+    v.out.tilesX = m->tilesX;
+    v.out.tilesY = m->tilesY;
+    v.out.zmin = m->zmin;
+    v.out.zmax = m->zmax;
+    v.out.vsinv = (float)(1.0 / (double)m->cfg.voxel_size);
+    v.out.rts = m->cfg.truncation / m->cfg.voxel_size;
+    v.out.mode = m->cfg.raycast_mode;
 }
+
+// Next render epoch of a map's z-range tiles; on wrap-around the tiles are
+// re-initialised (all-ones near, zero far) so no stale tag can match.
+cudaError_t next_epoch(vmap_map* m, cudaStream_t s, unsigned* epoch)
+{
+    if (m->epoch >= 0xFFFFFFFEu) {
+        const size_t nt = (size_t)m->tilesX * m->tilesY * sizeof(unsigned long long);
+        cudaError_t e = cudaMemsetAsync(m->zmin, 0xff, nt, s);
+        if (e == cudaSuccess) e = cudaMemsetAsync(m->zmax, 0, nt, s);
+        if (e != cudaSuccess) return e;
+        m->epoch = 0;
+    }
+    *epoch = ++m->epoch;
+    return cudaSuccess;
+}
+}  // namespace vmapb
+
+namespace {
 
 template <typename T>
 cudaError_t dalloc(vmap_map* m, T** p, size_t bytes)
@@ -301,8 +331,8 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
     VMAP_ALLOC(m->dm.pool, m->poolBytes);
     VMAP_ALLOC(m->dm.ctr, C_COUNT * sizeof(unsigned));
     VMAP_ALLOC(m->dm.visList, cap * sizeof(int));
-    VMAP_ALLOC(m->zmin, ntiles * sizeof(unsigned));
-    VMAP_ALLOC(m->zmax, ntiles * sizeof(unsigned));
+    VMAP_ALLOC(m->zmin, ntiles * sizeof(unsigned long long));
+    VMAP_ALLOC(m->zmax, ntiles * sizeof(unsigned long long));
     VMAP_ALLOC(m->dDepth, npix * sizeof(float));
     VMAP_ALLOC(m->dRgb, npix * 3);
     VMAP_ALLOC(m->dVmap, npix * sizeof(float4));
@@ -322,6 +352,7 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
     m->dm.vs = cfg.voxel_size;
     m->dm.mu = cfg.truncation;
     m->dm.wmax = (float)cfg.max_weight;
+    m->epoch = 0xFFFFFFFEu;  // the first render re-initialises the tiles
     vmap_status st = vmap_reset(m, nullptr);
     if (st == VMAP_OK && (e = cudaStreamSynchronize(nullptr)) != cudaSuccess) st = cuda_fail(e, "create sync");
     if (st != VMAP_OK) {
@@ -370,18 +401,20 @@ static vmap_status fuse_impl(vmap_map* m, const void* depth, int dtype, size_t d
         if (rgbPitch == 0) rgbPitch = 3 * (size_t)m->cfg.width;
         if (rgbPitch < 3 * (size_t)m->cfg.width) return VMAP_ERR_INVALID_ARG;
     }
-    FrameParams f;
-    make_frame(m, pose, f);
-    f.depth = depth;
-    f.dpitch = dpitch;
-    f.dtype = dtype;
-    f.dscale = dscale;
-    f.rgb = rgb;
-    f.rgbPitch = rgbPitch;
-    VMAP_CK(staged(m, VMAP_STAGE_ALLOC, s, [&] { return launch_alloc(m->dm, f, m->launcher, s); }));
-    VMAP_CK(staged(m, VMAP_STAGE_VISIBILITY, s, [&] { return launch_visibility(m->dm, f, m->launcher, s); }));
-    VMAP_CK(staged(m, VMAP_STAGE_FUSE, s,
-                   [&] { return launch_fuse(m->dm, m->cfg.voxel_format, rgb != nullptr, f, m->launcher, s); }));
+    OneView ov;
+    make_view(m, pose, ov.v);
+    ov.v.in.depth = depth;
+    ov.v.in.dpitch = dpitch;
+    ov.v.in.dtype = dtype;
+    ov.v.in.dscale = dscale;
+    ov.v.in.rgb = rgb;
+    ov.v.in.rgbPitch = rgbPitch;
+    ov.queue = m->dm.ctr + C_RAYQ;
+    const int tiles = tiles_32x8(m->cfg.width, m->cfg.height);
+    // alloc_kernel clears the visible counter the visibility kernel fills
+    VMAP_CK(staged(m, VMAP_STAGE_ALLOC, s, [&] { return launch_alloc(ov, tiles, m->launcher, s); }));
+    VMAP_CK(staged(m, VMAP_STAGE_VISIBILITY, s, [&] { return launch_visibility(ov, m->launcher, s); }));
+    VMAP_CK(staged(m, VMAP_STAGE_FUSE, s, [&] { return launch_fuse(ov, m->cfg.voxel_format, m->launcher, s); }));
     return VMAP_OK;
 }
 
@@ -418,10 +451,12 @@ vmap_status vmap_fuse_host(vmap_map* m, const void* depth_host, int depth_type, 
 vmap_status vmap_check_visible_blocks(vmap_map* m, const double pose[16], void* stream)
 {
     if (!m || !pose_ok(pose)) return VMAP_ERR_INVALID_ARG;
-    FrameParams f;
-    make_frame(m, pose, f);
+    OneView ov;
+    make_view(m, pose, ov.v);
+    ov.queue = m->dm.ctr + C_RAYQ;
     cudaStream_t s = as_stream(stream);
-    VMAP_CK(staged(m, VMAP_STAGE_VISIBILITY, s, [&] { return launch_visibility(m->dm, f, m->launcher, s); }));
+    VMAP_CK(cudaMemsetAsync(m->dm.ctr + C_VISIBLE, 0, sizeof(unsigned), s));
+    VMAP_CK(staged(m, VMAP_STAGE_VISIBILITY, s, [&] { return launch_visibility(ov, m->launcher, s); }));
     return VMAP_OK;
 }
 
@@ -436,36 +471,21 @@ vmap_status vmap_render_scene(vmap_map* m, const double pose[16], float* vmap_de
         ((uintptr_t)vmap_dev & 15) || ((uintptr_t)nmap_dev & 15))
         return VMAP_ERR_INVALID_ARG;
     cudaStream_t s = as_stream(stream);
-    RenderParams r;
-    r.W = m->cfg.width;
-    r.H = m->cfg.height;
-    r.fx = m->cfg.fx;
-    r.fy = m->cfg.fy;
-    r.cx = m->cfg.cx;
-    r.cy = m->cfg.cy;
-    r.ifx = (float)(1.0 / (double)m->cfg.fx);
-    r.ify = (float)(1.0 / (double)m->cfg.fy);
-    r.vsinv = (float)(1.0 / (double)m->cfg.voxel_size);
-    r.rts = m->cfg.truncation / m->cfg.voxel_size;
-    double inv[16];
-    vmap_pose_inverse(pose, inv);
-    to_xf(pose, r.T);
-    to_xf(inv, r.Ti);
-    r.mode = m->cfg.raycast_mode;
-    r.tilesX = m->tilesX;
-    r.tilesY = m->tilesY;
-    r.zmin = m->zmin;
-    r.zmax = m->zmax;
-    if (r.mode == 0)
-        VMAP_CK(staged(m, VMAP_STAGE_ZRANGE, s, [&] { return launch_zrange(m->dm, r, m->launcher, s); }));
-    VMAP_CK(staged(m, VMAP_STAGE_RAYCAST, s, [&] {
-        return launch_raycast(m->dm, m->cfg.voxel_format, r, reinterpret_cast<float4*>(vmap_dev), vmap_pitch,
-                              m->launcher, s);
-    }));
+    OneView ov;
+    make_view(m, pose, ov.v);
+    ov.queue = m->dm.ctr + C_RAYQ;
+    ov.v.out.vmap = reinterpret_cast<float4*>(vmap_dev);
+    ov.v.out.vpitch = vmap_pitch;
+    ov.v.out.nmap = reinterpret_cast<float4*>(nmap_dev);
+    ov.v.out.npitch = nmap_pitch;
+    VMAP_CK(next_epoch(m, s, &ov.v.out.epoch));
+    // the z-range kernel also rewinds the raycast work queue, so it runs in
+    // both raycast modes (with no work in mode 1)
+    VMAP_CK(staged(m, VMAP_STAGE_ZRANGE, s, [&] { return launch_zrange(ov, m->launcher, s); }));
+    VMAP_CK(staged(m, VMAP_STAGE_RAYCAST, s, [&] { return launch_raycast(ov, m->cfg.voxel_format, m->launcher, s); }));
     if (nmap_dev)
         VMAP_CK(staged(m, VMAP_STAGE_NORMALS, s, [&] {
-            return launch_normals(reinterpret_cast<const float4*>(vmap_dev), vmap_pitch,
-                                  reinterpret_cast<float4*>(nmap_dev), nmap_pitch, r.W, r.H, s);
+            return launch_normals(ov, tiles_32x8(m->cfg.width, m->cfg.height), m->launcher, s);
         }));
     return VMAP_OK;
 }
@@ -491,8 +511,19 @@ vmap_status vmap_compute_normal(const float* vmap_dev, size_t vmap_pitch, float*
     if (vmap_pitch == 0) vmap_pitch = row;
     if (nmap_pitch == 0) nmap_pitch = row;
     if (vmap_pitch < row || nmap_pitch < row || vmap_pitch % 16 || nmap_pitch % 16) return VMAP_ERR_INVALID_ARG;
-    VMAP_CK(launch_normals(reinterpret_cast<const float4*>(vmap_dev), vmap_pitch, reinterpret_cast<float4*>(nmap_dev),
-                           nmap_pitch, width, height, as_stream(stream)));
+    OneView ov;
+    std::memset(&ov, 0, sizeof(ov));
+    ov.v.cam.W = width;
+    ov.v.cam.H = height;
+    ov.v.out.vmap = const_cast<float4*>(reinterpret_cast<const float4*>(vmap_dev));
+    ov.v.out.vpitch = vmap_pitch;
+    ov.v.out.nmap = reinterpret_cast<float4*>(nmap_dev);
+    ov.v.out.npitch = nmap_pitch;
+    int dev = 0, sms = 1;
+    VMAP_CK(cudaGetDevice(&dev));
+    VMAP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    Launcher l{sms};
+    VMAP_CK(launch_normals(ov, tiles_32x8(width, height), l, as_stream(stream)));
     return VMAP_OK;
 }
 

@@ -39,6 +39,7 @@ enum {
     C_ERR = 2,     // VMAP_FLAG_* bits
     C_TRI = 3,     // triangles counted by the last polygonize
     C_FAILED = 4,  // allocations refused (pool full)
+    C_RAYQ = 8,    // raycast work queue of the single-map path
     C_COUNT = 16
 };
 
@@ -362,6 +363,111 @@ __device__ __forceinline__ void store_vec(void* dst, const void* src)
         for (int i = 0; i < NBYTES / 16; ++i)
             reinterpret_cast<uint4*>(dst)[i] = reinterpret_cast<const uint4*>(src)[i];
     }
+}
+
+}  // namespace vmapb
+
+namespace vmapb {
+
+// ------------------------------------------------------------- map views
+// Everything one stage kernel needs about one map for one step. Kernels are
+// written over a "view source": OneView (a single map, passed by value as the
+// kernel argument) or ManyViews (an array of views in device memory, one per
+// map of a batch). Work of a stage is split over the maps with per-map item
+// counts and a prefix sum computed at kernel start.
+struct CamParams {
+    int W, H;
+    float fx, fy, cx, cy;
+    float ifx, ify;  // (float)(1.0 / (double)f), as the reference's host code
+};
+
+struct FrameIn {
+    const void* depth;
+    size_t dpitch;
+    int dtype;       // VMAP_DEPTH_*
+    float dscale;    // uint16 -> metres
+    const uint8_t* rgb;  // uint8x3 per pixel or NULL
+    size_t rgbPitch;
+};
+
+struct RenderOut {
+    float4* vmap;
+    size_t vpitch;
+    float4* nmap;    // may be NULL
+    size_t npitch;
+    // tile depth bounds, tagged with the render epoch in the high word:
+    // zmin = (~epoch << 32 | float bits), folded with atomicMin; zmax =
+    // (epoch << 32 | float bits), folded with atomicMax. A newer epoch always
+    // wins, so the tiles never need clearing between renders.
+    unsigned long long* zmin;
+    unsigned long long* zmax;
+    unsigned epoch;  // 1 .. 2^32 - 2
+    int tilesX, tilesY;
+    float vsinv;     // (float)(1.0 / (double)voxel_size)
+    float rts;       // truncation / voxel_size (raytraceStep)
+    int mode;        // 0: z-range bounded, 1: full march
+};
+
+struct MapView {
+    DevMap m;
+    CamParams cam;
+    FrameIn in;
+    RenderOut out;
+    Xf T;   // camera -> world
+    Xf Ti;  // world -> camera
+};
+
+constexpr int kMaxBatch = 256;
+
+struct OneView {
+    MapView v;
+    unsigned* queue;  // work-queue counters of this step
+    __device__ __forceinline__ int count() const { return 1; }
+    __device__ __forceinline__ const MapView& operator[](int) const { return v; }
+};
+
+struct ManyViews {
+    const MapView* v;
+    int n;
+    unsigned* queue;
+    __device__ __forceinline__ int count() const { return n; }
+    __device__ __forceinline__ const MapView& operator[](int i) const { return v[i]; }
+};
+
+// Exclusive prefix of per-map item counts in shared memory (pre[0..n]),
+// computed by the first warp; the CTA must call it uniformly.
+template <class V, class F>
+__device__ __forceinline__ void map_prefix(const V& views, F items, int* pre)
+{
+    const int n = views.count();
+    if (threadIdx.x < 32) {
+        int run = 0;
+        for (int base = 0; base < n; base += 32) {
+            const int i = base + (int)threadIdx.x;
+            int v = i < n ? items(views[i]) : 0;
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, v, d);
+                if ((int)threadIdx.x >= d) v += u;
+            }
+            if (i < n) pre[i + 1] = run + v;
+            run += __shfl_sync(0xffffffffu, v, 31);
+        }
+        if (threadIdx.x == 0) pre[0] = 0;
+    }
+    __syncthreads();
+}
+
+// Map owning item i: largest m with pre[m] <= i (pre is non-decreasing).
+__device__ __forceinline__ int map_of(const int* pre, int n, int i)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (pre[mid] <= i) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
 }
 
 }  // namespace vmapb

@@ -172,6 +172,17 @@ class VoxelMapping:
     def clear_errors(self):
         L.check(self._lib.vmap_clear_errors(self._need(), _stream()))
 
+    def export_blocks_static(self, first, count):
+        """vmap_export_blocks_static: at most 256 blocks, no allocation."""
+        coords = np.zeros((count, 3), np.int32)
+        tsdf = np.zeros((count, 512), np.float32)
+        weight = np.zeros((count, 512), np.float32)
+        got = C.c_uint32()
+        L.check(self._lib.vmap_export_blocks_static(self._need(), first, count, coords.ctypes.data, tsdf.ctypes.data,
+                                                    weight.ctypes.data, None, C.byref(got), _stream()))
+        k = got.value
+        return {"coords": coords[:k], "tsdf": tsdf[:k], "weight": weight[:k]}
+
     def export_blocks(self, with_rgb=None):
         """Allocated blocks in pool order: coords (n, 3) int32, tsdf / weight
         (n, 512) float32 (voxel x + 8y + 64z), rgb (n, 512, 3) uint8 or None."""
@@ -186,3 +197,55 @@ class VoxelMapping:
         L.check(self._lib.vmap_export_blocks(self._map, cp(coords), cp(tsdf), cp(weight), cp(rgb), n,
                                              C.byref(got), _stream()), "vmap_export_blocks")
         return {"coords": coords, "tsdf": tsdf, "weight": weight, "rgb": rgb}
+
+
+class MapBatch:
+    """Fuse + raycast many VoxelMapping maps per step (vmap_batch_*).
+
+    step(depths, rgbs, poses, vmaps, nmaps) fuses depths[i] (and rgbs[i]) into
+    maps[i] at poses[i] and raycasts maps[i] at the same pose into vmaps[i]
+    (and nmaps[i]); every stage is one launch over all maps, replayed as a CUDA
+    graph from the third step on (non-default streams)."""
+
+    def __init__(self, maps):
+        self.maps = list(maps)
+        self._lib = L.lib()
+        arr = (C.c_void_p * len(self.maps))(*[m._need().value for m in self.maps])
+        h = C.c_void_p()
+        L.check(self._lib.vmap_batch_create(arr, len(self.maps), C.byref(h)), "vmap_batch_create")
+        self._h = h
+        self._frames = (L.BatchFrame * len(self.maps))()
+
+    def release(self):
+        if getattr(self, "_h", None) is not None:
+            L.check(self._lib.vmap_batch_destroy(self._h), "vmap_batch_destroy")
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+    def step(self, depths, rgbs, poses, vmaps, nmaps=None, depth_scale=0.001, stream=None):
+        import torch
+        for i, m in enumerate(self.maps):
+            f = self._frames[i]
+            d = depths[i]
+            f.depth_dev = d.data_ptr()
+            f.depth_type = L.DEPTH_U16 if d.dtype in (torch.uint16, torch.int16) else L.DEPTH_F32
+            f.depth_pitch = d.stride(0) * d.element_size()
+            f.depth_scale = depth_scale
+            c = rgbs[i] if rgbs is not None else None
+            f.rgb_dev = c.data_ptr() if c is not None else None
+            f.rgb_pitch = c.stride(0) * c.element_size() if c is not None else 0
+            p = np.asarray(poses[i], np.float64).reshape(16)
+            for k in range(16):
+                f.pose[k] = p[k]
+            f.vmap_dev = vmaps[i].data_ptr()
+            f.vmap_pitch = vmaps[i].stride(0) * 4
+            n = nmaps[i] if nmaps is not None else None
+            f.nmap_dev = n.data_ptr() if n is not None else None
+            f.nmap_pitch = n.stride(0) * 4 if n is not None else 0
+        s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
+        L.check(self._lib.vmap_batch_step(self._h, self._frames, s), "vmap_batch_step")
