@@ -273,8 +273,7 @@ __global__ void reset_hash_kernel(DevMap m)
 {
     const size_t n = (size_t)m.nBucket * kSlots;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-        m.keys[i] = kEmptyKey;
-        m.vals[i] = -1;
+        m.slots[i] = make_ulonglong2(kEmptyKey, ~0ull);
     }
 }
 

@@ -160,8 +160,7 @@ cudaError_t staged(vmap_map* m, int stage, cudaStream_t s, F&& launch)
 void free_all(vmap_map* m)
 {
     timing_free(m);
-    cudaFree(m->dm.keys);
-    cudaFree(m->dm.vals);
+    cudaFree(m->dm.slots);
     cudaFree(m->dm.blockKeys);
     cudaFree(m->dm.pool);
     cudaFree(m->dm.ctr);
@@ -325,8 +324,7 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
             return st;                                                \
         }                                                             \
     } while (0)
-    VMAP_ALLOC(m->dm.keys, nslots * sizeof(unsigned long long));
-    VMAP_ALLOC(m->dm.vals, nslots * sizeof(int));
+    VMAP_ALLOC(m->dm.slots, nslots * sizeof(ulonglong2));
     VMAP_ALLOC(m->dm.blockKeys, cap * sizeof(unsigned long long));
     VMAP_ALLOC(m->dm.pool, m->poolBytes);
     VMAP_ALLOC(m->dm.ctr, C_COUNT * sizeof(unsigned));

@@ -20,8 +20,7 @@
 //     and steps 1 voxel at a time, the steps up to the block's exit are taken
 //     as one integer jump;
 //   * block lookups are cached per thread.
-// The ray kernel is persistent: its warps take 8x4-pixel tiles of every map
-// of the batch from one device-side queue until the queue runs dry.
+// The ray marcher itself lives in raymarch.cu.
 #include "vmap_launch.h"
 
 namespace vmapb {
@@ -101,216 +100,6 @@ __global__ void __launch_bounds__(256) zrange_kernel(V views)
                 atomicMin(r.zmin + t, lo);
                 atomicMax(r.zmax + t, hi);
             }
-    }
-}
-
-// ------------------------------------------------------------------ raycast
-template <int FMT>
-struct RayCtx {
-    const DevMap& m;
-    int cbx, cby, cbz, cblk;  // block of the current sample
-    int obx, oby, obz, oblk;  // last other block (trilinear corners)
-
-    __device__ __forceinline__ RayCtx(const DevMap& mm)
-        : m(mm), cbx(INT_MIN), cby(0), cbz(0), cblk(-1), obx(INT_MIN), oby(0), obz(0), oblk(-1)
-    {
-    }
-
-    __device__ __forceinline__ int block_of(int bx, int by, int bz)
-    {
-        if (bx == cbx && by == cby && bz == cbz) return cblk;
-        if (bx == obx && by == oby && bz == obz) return oblk;
-        obx = bx;
-        oby = by;
-        obz = bz;
-        oblk = hash_find(m, bx, by, bz);
-        return oblk;
-    }
-
-    // read_sdf (ray_tracing.cu:272-286): voxel at integer coordinates;
-    // unallocated or zero weight -> invalid, 1.0
-    __device__ __forceinline__ float voxel(int slot, int vx, int vy, int vz, bool& valid) const
-    {
-        if (slot >= 0) {
-            const typename Fmt<FMT>::Word w = __ldg(Layout<FMT>::words(m, slot) + local_idx(vx, vy, vz));
-            if (Fmt<FMT>::observed(w)) {
-                valid = true;
-                return Fmt<FMT>::tsdf(w);
-            }
-        }
-        valid = false;
-        return 1.f;
-    }
-
-    // read_sdf_interped (ray_tracing.cu:288-321). When `have0` is set, s0/v0
-    // are the value and validity of corner 0 (the voxel at floor(p)), already
-    // read by the caller.
-    __device__ float interp(float3 p, bool& valid, bool have0 = false, float s0 = 1.f, bool v0 = false)
-    {
-        const float flx = floorf(p.x), fly = floorf(p.y), flz = floorf(p.z);
-        const float ax = __fsub_rn(p.x, flx), ay = __fsub_rn(p.y, fly), az = __fsub_rn(p.z, flz);
-        const int x0 = __float2int_rz(flx), y0 = __float2int_rz(fly), z0 = __float2int_rz(flz);
-        const int x1 = __float2int_rz(floorf(__fadd_rn(p.x, 1.f)));
-        const int y1 = __float2int_rz(floorf(__fadd_rn(p.y, 1.f)));
-        const int z1 = __float2int_rz(floorf(__fadd_rn(p.z, 1.f)));
-        float s[8];
-        bool ok = true;
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            bool v;
-            if (c == 0 && have0) {
-                s[0] = s0;
-                v = v0;
-            } else {
-                const int vx = (c & 1) ? x1 : x0, vy = (c & 2) ? y1 : y0, vz = (c & 4) ? z1 : z0;
-                s[c] = voxel(block_of(vox2blk(vx), vox2blk(vy), vox2blk(vz)), vx, vy, vz, v);
-            }
-            ok &= v;
-        }
-        const float bx = __fsub_rn(1.f, ax), by = __fsub_rn(1.f, ay), bz = __fsub_rn(1.f, az);
-        const float r0 = __fmaf_rn(bx, s[0], __fmul_rn(ax, s[1]));
-        const float r1 = __fmaf_rn(bx, s[2], __fmul_rn(ax, s[3]));
-        const float r2 = __fmaf_rn(by, r0, __fmul_rn(ay, r1));
-        const float r4 = __fmaf_rn(bx, s[4], __fmul_rn(ax, s[5]));
-        const float r5 = __fmaf_rn(bx, s[6], __fmul_rn(ax, s[7]));
-        const float r3 = __fmaf_rn(by, r4, __fmul_rn(ay, r5));
-        valid = ok;
-        return __fmaf_rn(bz, r2, __fmul_rn(az, r3));
-    }
-};
-
-__device__ __forceinline__ float3 fma3(float k, float3 d, float3 r)
-{
-    return make_float3(__fmaf_rn(k, d.x, r.x), __fmaf_rn(k, d.y, r.y), __fmaf_rn(k, d.z, r.z));
-}
-
-// MapRenderingDelegate::operator() (ray_tracing.cu:323-400) for pixel (x, y).
-template <int FMT>
-__device__ __forceinline__ void trace_ray(const MapView& v, int x, int y)
-{
-    const RenderOut& r = v.out;
-    const CamParams& c = v.cam;
-    float4* out = reinterpret_cast<float4*>(reinterpret_cast<char*>(r.vmap) + (size_t)y * r.vpitch) + x;
-    const float qnan = __int_as_float(0x7fffffff);
-    const float4 miss = make_float4(qnan, qnan, qnan, qnan);
-
-    float zn = 0.f, zf = kMaxDepth;
-    if (r.mode == 0) {
-        const int t = (y >> 3) * r.tilesX + (x >> 3);
-        const unsigned long long kn = __ldg(r.zmin + t), kf = __ldg(r.zmax + t);
-        if ((unsigned)(kn >> 32) != ~r.epoch || (unsigned)(kf >> 32) != r.epoch) {
-            *out = miss;  // no allocated block projects into this tile
-            return;
-        }
-        zn = __uint_as_float((unsigned)kn);
-        zf = __uint_as_float((unsigned)kf);
-    }
-
-    const float3 p0 = unproject(x, y, kMinDepth, c.ifx, c.ify, c.cx, c.cy);
-    const float dist0 = __fmul_rn(__fsqrt_rn(sqnorm(p0)), r.vsinv);
-    float3 bs = xf_apply(v.T, p0.x, p0.y, p0.z);
-    bs = make_float3(__fmul_rn(bs.x, r.vsinv), __fmul_rn(bs.y, r.vsinv), __fmul_rn(bs.z, r.vsinv));
-    const float3 p1 = unproject(x, y, kMaxDepth, c.ifx, c.ify, c.cx, c.cy);
-    const float dist_e = __fmul_rn(__fsqrt_rn(sqnorm(p1)), r.vsinv);
-    float3 be = xf_apply(v.T, p1.x, p1.y, p1.z);
-    be = make_float3(__fmul_rn(be.x, r.vsinv), __fmul_rn(be.y, r.vsinv), __fmul_rn(be.z, r.vsinv));
-    const float3 dir = normalized(make_float3(__fsub_rn(be.x, bs.x), __fsub_rn(be.y, bs.y), __fsub_rn(be.z, bs.z)));
-    // exit faces: +8 along axes the ray runs up (and +0), +0 along axes it runs
-    // down (and -0), so a zero component gives an infinite exit distance
-    const float3 inv = make_float3(__frcp_rn(dir.x), __frcp_rn(dir.y), __frcp_rn(dir.z));
-    const int ox = signbit(dir.x) ? 0 : 8, oy = signbit(dir.y) ? 0 : 8, oz = signbit(dir.z) ? 0 : 8;
-
-    float3 res = bs;
-    float dist_s = dist0;
-    float dist_lim = dist_e;
-    if (r.mode == 0) {
-        // ray length (voxels) is proportional to camera depth along a ray
-        const float g = dist_e / kMaxDepth;
-        const float k0 = floorf(g * zn - dist0) - 2.f;
-        if (k0 > 0.f) {
-            res = fma3(k0, dir, res);
-            dist_s = dist0 + k0;
-        }
-        dist_lim = fminf(dist_e, g * zf + 2.f);
-    }
-
-    RayCtx<FMT> ctx(v.m);
-    float sdf = 1.f, step;
-    bool valid = false;
-    while (dist_s < dist_lim) {
-        const float flx = floorf(res.x), fly = floorf(res.y), flz = floorf(res.z);
-        const int vx = __float2int_rz(flx), vy = __float2int_rz(fly), vz = __float2int_rz(flz);
-        const int bx = vox2blk(vx), by = vox2blk(vy), bz = vox2blk(vz);
-        if (bx != ctx.cbx || by != ctx.cby || bz != ctx.cbz) {
-            const int s = (bx == ctx.obx && by == ctx.oby && bz == ctx.obz) ? ctx.oblk : hash_find(v.m, bx, by, bz);
-            ctx.cbx = bx;
-            ctx.cby = by;
-            ctx.cbz = bz;
-            ctx.cblk = s;
-        }
-        if (ctx.cblk < 0) {
-            // every 1-voxel step inside this unallocated block reads (1.0, invalid):
-            // jump to the last step that is still inside (at least one step)
-            const float tx = ((float)(bx * 8 + ox) - res.x) * inv.x;
-            const float ty = ((float)(by * 8 + oy) - res.y) * inv.y;
-            const float tz = ((float)(bz * 8 + oz) - res.z) * inv.z;
-            const float t = fminf(fminf(tx, ty), tz);  // fminf drops the NaN of 0 * inf
-            const float k = fmaxf(1.f, ceilf(t - 1e-3f));
-            res = fma3(k, dir, res);
-            dist_s = __fadd_rn(dist_s, k);
-            sdf = 1.f;
-            valid = false;
-            continue;
-        }
-        sdf = ctx.voxel(ctx.cblk, vx, vy, vz, valid);
-        if (sdf <= 0.5f && sdf >= -0.5f) sdf = ctx.interp(res, valid, true, sdf, valid);
-        if (sdf <= 0.f) break;
-        step = valid ? fmaxf(__fmul_rn(sdf, r.rts), 1.f) : 1.f;
-        res = fma3(step, dir, res);
-        dist_s = __fadd_rn(dist_s, step);
-    }
-
-    bool found = false;
-    if (sdf <= 0.f) {
-        step = __fmul_rn(sdf, r.rts);
-        res = fma3(step, dir, res);
-        sdf = ctx.interp(res, valid);
-        step = __fmul_rn(sdf, r.rts);
-        res = fma3(step, dir, res);
-        found = valid;
-    }
-    if (found) {
-        const float3 o = xf_apply(v.Ti, __fdiv_rn(res.x, r.vsinv), __fdiv_rn(res.y, r.vsinv), __fdiv_rn(res.z, r.vsinv));
-        *out = make_float4(o.x, o.y, o.z, 1.f);
-    } else {
-        *out = miss;
-    }
-}
-
-__device__ __forceinline__ int ray_tiles(const MapView& v) { return ((v.cam.W + 7) >> 3) * ((v.cam.H + 3) >> 2); }
-
-// Persistent: each warp takes one 8x4-pixel tile at a time from the queue
-// (rewound by zrange_kernel) until every tile of every map is done.
-template <class V, int FMT>
-__global__ void __launch_bounds__(256) raycast_kernel(V views)
-{
-    __shared__ int pre[kMaxBatch + 1];
-    map_prefix(views, [](const MapView& v) { return ray_tiles(v); }, pre);
-    const int nmaps = views.count();
-    const int total = pre[nmaps];
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        int item = 0;
-        if (lane == 0) item = (int)atomicAdd(views.queue, 1u);
-        item = __shfl_sync(0xffffffffu, item, 0);
-        if (item >= total) break;
-        const int mi = map_of(pre, nmaps, item);
-        const MapView& v = views[mi];
-        const int t = item - pre[mi];
-        const int tx = (v.cam.W + 7) >> 3;
-        const int x = (t % tx) * 8 + (lane & 7);
-        const int y = (t / tx) * 4 + (lane >> 3);
-        if (x < v.cam.W && y < v.cam.H) trace_ray<FMT>(v, x, y);
     }
 }
 
@@ -397,30 +186,6 @@ cudaError_t launch_zrange(const V& views, const Launcher& l, cudaStream_t s)
     return cudaGetLastError();
 }
 
-template <class V, int FMT>
-static cudaError_t raycast_persistent(const V& views, const Launcher& l, cudaStream_t s)
-{
-    static int occ = 0;  // resident CTAs per SM of this instantiation
-    if (occ == 0) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, raycast_kernel<V, FMT>, 256, 0);
-        if (e != cudaSuccess || occ < 1) occ = 1;
-    }
-    raycast_kernel<V, FMT><<<l.numSMs * occ, 256, 0, s>>>(views);
-    return cudaGetLastError();
-}
-
-template <class V>
-cudaError_t launch_raycast(const V& views, int fmt, const Launcher& l, cudaStream_t s)
-{
-    switch (fmt) {
-    case VMAP_VOXEL_REF: return raycast_persistent<V, VMAP_VOXEL_REF>(views, l, s);
-    case VMAP_VOXEL_F32: return raycast_persistent<V, VMAP_VOXEL_F32>(views, l, s);
-    case VMAP_VOXEL_F16: return raycast_persistent<V, VMAP_VOXEL_F16>(views, l, s);
-    case VMAP_VOXEL_I16: return raycast_persistent<V, VMAP_VOXEL_I16>(views, l, s);
-    default: return cudaErrorInvalidValue;
-    }
-}
-
 template <class V>
 cudaError_t launch_normals(const V& views, int totalTiles, const Launcher& l, cudaStream_t s)
 {
@@ -431,8 +196,6 @@ cudaError_t launch_normals(const V& views, int totalTiles, const Launcher& l, cu
 
 template cudaError_t launch_zrange<OneView>(const OneView&, const Launcher&, cudaStream_t);
 template cudaError_t launch_zrange<ManyViews>(const ManyViews&, const Launcher&, cudaStream_t);
-template cudaError_t launch_raycast<OneView>(const OneView&, int, const Launcher&, cudaStream_t);
-template cudaError_t launch_raycast<ManyViews>(const ManyViews&, int, const Launcher&, cudaStream_t);
 template cudaError_t launch_normals<OneView>(const OneView&, int, const Launcher&, cudaStream_t);
 template cudaError_t launch_normals<ManyViews>(const ManyViews&, int, const Launcher&, cudaStream_t);
 

@@ -49,8 +49,7 @@ struct Xf {
 };
 
 struct DevMap {
-    unsigned long long* keys;      // nBucket * kSlots packed block coordinates
-    int* vals;                     // nBucket * kSlots pool slot (or -1)
+    ulonglong2* slots;             // nBucket * kSlots: {packed block coordinates, pool slot or -1}
     unsigned long long* blockKeys; // capacity: key of each allocated block
     unsigned char* pool;           // capacity * blockBytes
     unsigned* ctr;                 // C_COUNT counters
@@ -189,7 +188,8 @@ __device__ __forceinline__ bool block_visible(int bx, int by, int bz, const Xf& 
 
 // ------------------------------------------------------------- hash table
 // Bucketed open hashing: bucket = reference hash of the block coordinates,
-// 4 slots per bucket (one 32-byte sector), linear probing into the next
+// 4 slots per bucket (key and pool slot side by side: one 64-byte read per
+// probe, no second round trip for the value), linear probing into the next
 // bucket when all 4 are taken. Slots go EMPTY -> key exactly once, so the
 // filled slots of a bucket always form a prefix: a lookup stops at the first
 // EMPTY slot.
@@ -200,17 +200,16 @@ __device__ __forceinline__ int hash_find(const DevMap& m, int bx, int by, int bz
     int b = ref_hash_fast(bx, by, bz, m.nBucket, m.bucketMagic);
 #pragma unroll 1
     for (int p = 0; p < kMaxProbe; ++p) {
-        const ulonglong2* s = reinterpret_cast<const ulonglong2*>(m.keys + (size_t)b * kSlots);
-        const ulonglong2 k01 = __ldg(s), k23 = __ldg(s + 1);
-        const int base = b * kSlots;
-        if (k01.x == key) return __ldg(m.vals + base);
-        if (k01.x == kEmptyKey) return -1;
-        if (k01.y == key) return __ldg(m.vals + base + 1);
-        if (k01.y == kEmptyKey) return -1;
-        if (k23.x == key) return __ldg(m.vals + base + 2);
-        if (k23.x == kEmptyKey) return -1;
-        if (k23.y == key) return __ldg(m.vals + base + 3);
-        if (k23.y == kEmptyKey) return -1;
+        const ulonglong2* s = m.slots + (size_t)b * kSlots;
+        const ulonglong2 a0 = __ldg(s), a1 = __ldg(s + 1), a2 = __ldg(s + 2), a3 = __ldg(s + 3);
+        if (a0.x == key) return (int)a0.y;
+        if (a0.x == kEmptyKey) return -1;
+        if (a1.x == key) return (int)a1.y;
+        if (a1.x == kEmptyKey) return -1;
+        if (a2.x == key) return (int)a2.y;
+        if (a2.x == kEmptyKey) return -1;
+        if (a3.x == key) return (int)a3.y;
+        if (a3.x == kEmptyKey) return -1;
         b = (b + 1 == m.nBucket) ? 0 : b + 1;
     }
     return -1;
@@ -226,14 +225,12 @@ __device__ __forceinline__ void hash_insert(const DevMap& m, int bx, int by, int
     int b = ref_hash_fast(bx, by, bz, m.nBucket, m.bucketMagic);
 #pragma unroll 1
     for (int p = 0; p < kMaxProbe; ++p) {
-        unsigned long long* s = m.keys + (size_t)b * kSlots;
-        const ulonglong2 k01 = __ldcg(reinterpret_cast<const ulonglong2*>(s));
-        const ulonglong2 k23 = __ldcg(reinterpret_cast<const ulonglong2*>(s) + 1);
-        const unsigned long long k[4] = {k01.x, k01.y, k23.x, k23.y};
+        ulonglong2* s = m.slots + (size_t)b * kSlots;
+        const unsigned long long k[4] = {__ldcg(&s[0].x), __ldcg(&s[1].x), __ldcg(&s[2].x), __ldcg(&s[3].x)};
 #pragma unroll
         for (int i = 0; i < kSlots; ++i) {
             unsigned long long cur = k[i];
-            if (cur == kEmptyKey) cur = atomicCAS(s + i, kEmptyKey, key);
+            if (cur == kEmptyKey) cur = atomicCAS(&s[i].x, kEmptyKey, key);
             if (cur == key) return;  // present (or inserted by another thread)
             if (cur == kEmptyKey) {  // this thread won the slot
                 cg::coalesced_group g = cg::coalesced_threads();
@@ -242,7 +239,7 @@ __device__ __forceinline__ void hash_insert(const DevMap& m, int bx, int by, int
                 const unsigned slot = g.shfl(first, 0) + g.thread_rank();
                 if (slot < (unsigned)m.capacity) {
                     m.blockKeys[slot] = key;
-                    m.vals[(size_t)b * kSlots + i] = (int)slot;
+                    s[i].y = (unsigned long long)slot;
                 } else {
                     atomicOr(m.ctr + C_ERR, VMAP_FLAG_POOL_FULL);
                     atomicAdd(m.ctr + C_FAILED, 1u);
