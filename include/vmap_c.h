@@ -179,15 +179,18 @@ vmap_status vmap_surface_points(const float* verts_dev, uint32_t n_tris, float* 
  * batch share one voxel format. A map may belong to several batches but only
  * one step may use it at a time. */
 typedef struct vmap_batch vmap_batch;
+/* A NULL depth_dev skips the map's fusion this step (rgb_dev must then be
+ * NULL), a NULL vmap_dev its render (nmap_dev must then be NULL); with both
+ * NULL the map is idle for the step. */
 typedef struct vmap_batch_frame {
-    const void* depth_dev;   /* map-sized depth image                        */
+    const void* depth_dev;   /* map-sized depth image or NULL (no fusion)    */
     int depth_type;          /* vmap_depth_type                              */
     size_t depth_pitch;      /* bytes, 0 = packed                            */
     float depth_scale;       /* uint16 -> metres                             */
     const uint8_t* rgb_dev;  /* uint8x3 or NULL (no colour this step)        */
     size_t rgb_pitch;
     double pose[16];         /* camera-to-world, row-major                   */
-    float* vmap_dev;         /* float4 vertex map out, 16-byte aligned       */
+    float* vmap_dev;         /* float4 vertex map out (16-byte aligned) or NULL */
     size_t vmap_pitch;
     float* nmap_dev;         /* float4 normal map out or NULL                */
     size_t nmap_pitch;

@@ -86,3 +86,56 @@ def test_batch_rejects_mixed_formats_and_duplicates():
         MapBatch([a, b])
     with pytest.raises(L.VmapError):
         MapBatch([a, a])
+
+
+def test_batch_fuse_only_and_render_only_frames():
+    """A step may fuse some maps, render others and leave the rest idle: the
+    result equals the matching single-map calls, and idle maps keep their
+    visible count."""
+    wls = workloads()
+    scenes = [synth.Scene(wl) for wl in wls]
+    batch_maps = [make_map(wl) for wl in wls]
+    solo_maps = [make_map(wl) for wl in wls]
+    batch = MapBatch(batch_maps)
+    side = torch.cuda.Stream()
+    # (fuse, render) per map and step; step 0 fuses everything so renders see surface
+    plan = [[(1, 1), (1, 1), (1, 1)], [(1, 0), (0, 1), (0, 0)], [(0, 1), (1, 0), (1, 1)],
+            [(0, 0), (1, 1), (0, 1)], [(1, 0), (0, 0), (1, 0)]]
+    for step, work in enumerate(plan):
+        depths, rgbs, poses, vb, nb = [], [], [], [], []
+        for (fu, re), wl, sc in zip(work, wls, scenes):
+            d, c, p = sc.render(step * 4)
+            depths.append(torch.from_numpy(d.view(np.int16)).cuda() if fu else None)
+            rgbs.append(torch.from_numpy(c).cuda().reshape(wl.height, -1) if fu and wl.with_color else None)
+            poses.append(p)
+            vb.append(torch.full((wl.height, wl.width, 4), 7.0, device="cuda") if re else None)
+            nb.append(torch.full((wl.height, wl.width, 4), 7.0, device="cuda") if re else None)
+        vis_before = [m.stats()["visible_blocks"] for m in batch_maps]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            batch.step(depths, rgbs, poses, vb, nb)
+        side.synchronize()
+        for i, ((fu, re), wl, vm) in enumerate(zip(work, wls, solo_maps)):
+            if fu:
+                if wl.with_color:
+                    vm.FuseDepthAndImage(rgbs[i], depths[i], poses[i])
+                else:
+                    vm.FuseDepth(depths[i], poses[i])
+                assert batch_maps[i].stats()["visible_blocks"] == vm.stats()["visible_blocks"], (step, i)
+            else:
+                assert batch_maps[i].stats()["visible_blocks"] == vis_before[i], (step, i)
+            if re:
+                nm = torch.empty_like(vb[i])
+                v = vm.RenderScene(None, poses[i], nmap=nm)
+                torch.cuda.synchronize()
+                assert np.array_equal(np.nan_to_num(v.cpu().numpy(), nan=-9.0),
+                                      np.nan_to_num(vb[i].cpu().numpy(), nan=-9.0)), (step, i)
+                assert np.array_equal(np.nan_to_num(nm.cpu().numpy(), nan=-9.0),
+                                      np.nan_to_num(nb[i].cpu().numpy(), nan=-9.0)), (step, i)
+    for wl, a, b in zip(wls, batch_maps, solo_maps):
+        ea, eb = a.export_blocks(), b.export_blocks()
+        ia, ib = np.argsort(block_keys(ea["coords"])), np.argsort(block_keys(eb["coords"]))
+        for k in ("coords", "tsdf", "weight") + (("rgb",) if wl.with_color else ()):
+            assert np.array_equal(ea[k][ia], eb[k][ib]), k
+        assert a.stats()["error_flags"] == 0
+    batch.release()

@@ -154,23 +154,29 @@ vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void*
         vmap_map* m = b->maps[i];
         vmap_config c;
         vmap_get_config(m, &c);
-        bool ok = f.depth_dev && f.vmap_dev && (f.depth_type == VMAP_DEPTH_F32 || f.depth_type == VMAP_DEPTH_U16);
+        // a NULL depth frame skips this map's fusion, a NULL vertex map its
+        // render; a frame with neither leaves the map idle for the step
+        const bool fuse = f.depth_dev != nullptr, render = f.vmap_dev != nullptr;
+        bool ok = (!fuse || f.depth_type == VMAP_DEPTH_F32 || f.depth_type == VMAP_DEPTH_U16) &&
+                  (render || !f.nmap_dev) && (fuse || !f.rgb_dev);
         for (int k = 0; k < 12 && ok; ++k) ok = std::isfinite(f.pose[k]);
         const size_t elem = f.depth_type == VMAP_DEPTH_F32 ? 4 : 2;
         const size_t dp = f.depth_pitch ? f.depth_pitch : elem * c.width;
         const size_t row = sizeof(float4) * (size_t)c.width;
         const size_t vp = f.vmap_pitch ? f.vmap_pitch : row, np = f.nmap_pitch ? f.nmap_pitch : row;
         const size_t rp = f.rgb_pitch ? f.rgb_pitch : 3 * (size_t)c.width;
-        ok = ok && dp >= elem * c.width && dp % elem == 0 && vp >= row && vp % 16 == 0 &&
-             ((uintptr_t)f.vmap_dev & 15) == 0 && (!f.nmap_dev || (np >= row && np % 16 == 0)) &&
-             ((uintptr_t)f.nmap_dev & 15) == 0 && (!f.rgb_dev || (c.with_color && rp >= 3 * (size_t)c.width)) &&
-             (f.depth_type != VMAP_DEPTH_U16 || f.depth_scale > 0);
+        ok = ok && (!fuse || (dp >= elem * c.width && dp % elem == 0 &&
+                              (f.depth_type != VMAP_DEPTH_U16 || f.depth_scale > 0))) &&
+             (!render || (vp >= row && vp % 16 == 0 && ((uintptr_t)f.vmap_dev & 15) == 0)) &&
+             (!f.nmap_dev || (np >= row && np % 16 == 0)) && ((uintptr_t)f.nmap_dev & 15) == 0 &&
+             (!f.rgb_dev || (c.with_color && rp >= 3 * (size_t)c.width));
         if (!ok) {
             set_last_error("vmap_batch_step: invalid frame " + std::to_string(i));
             return VMAP_ERR_INVALID_ARG;
         }
         MapView& v = b->hViews[buf][i];
         make_view(m, f.pose, v);
+        v.in.active = fuse;
         v.in.depth = f.depth_dev;
         v.in.dpitch = dp;
         v.in.dtype = f.depth_type;
@@ -181,7 +187,7 @@ vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void*
         v.out.vpitch = vp;
         v.out.nmap = reinterpret_cast<float4*>(f.nmap_dev);
         v.out.npitch = np;
-        VMAP_BCK(next_epoch(m, s, &v.out.epoch));
+        if (render) VMAP_BCK(next_epoch(m, s, &v.out.epoch));
     }
     const size_t bytes = sizeof(MapView) * (size_t)n;
     if (s == nullptr) {  // the legacy stream cannot be captured: launch directly

@@ -27,7 +27,11 @@ __device__ __forceinline__ float read_depth(const FrameIn& f, int x, int y)
     return f.dtype == VMAP_DEPTH_U16 ? read_depth_t<VMAP_DEPTH_U16>(f, x, y) : read_depth_t<VMAP_DEPTH_F32>(f, x, y);
 }
 
-__device__ __forceinline__ int alloc_tiles(const MapView& v) { return ((v.cam.W + 31) >> 5) * ((v.cam.H + 7) >> 3); }
+// maps without fusion work this step (no frame) contribute no items
+__device__ __forceinline__ int alloc_tiles(const MapView& v)
+{
+    return v.in.active ? ((v.cam.W + 31) >> 5) * ((v.cam.H + 7) >> 3) : 0;
+}
 
 // ---------------------------------------------------------------- allocation
 // One thread per depth pixel, a 256-thread CTA per 32x8-pixel tile
@@ -45,7 +49,8 @@ __global__ void __launch_bounds__(256) alloc_kernel(V views)
     map_prefix(views, [](const MapView& v) { return alloc_tiles(v); }, pre);
     const int nmaps = views.count();
     if (blockIdx.x == 0)
-        for (int i = threadIdx.x; i < nmaps; i += blockDim.x) views[i].m.ctr[C_VISIBLE] = 0u;
+        for (int i = threadIdx.x; i < nmaps; i += blockDim.x)
+            if (views[i].in.active) views[i].m.ctr[C_VISIBLE] = 0u;
     const int total = pre[nmaps];
     const int lane = threadIdx.x & 31;
     for (int item = blockIdx.x; item < total; item += gridDim.x) {
@@ -136,7 +141,7 @@ template <class V>
 __global__ void __launch_bounds__(256) visibility_kernel(V views)
 {
     __shared__ int pre[kMaxBatch + 1];
-    map_prefix(views, [](const MapView& v) { return (allocated_blocks(v.m) + 31) >> 5; }, pre);
+    map_prefix(views, [](const MapView& v) { return v.in.active ? (allocated_blocks(v.m) + 31) >> 5 : 0; }, pre);
     const int nmaps = views.count();
     const int total = pre[nmaps];
     const int lane = threadIdx.x & 31;
@@ -246,7 +251,7 @@ template <class V, int FMT>
 __global__ void __launch_bounds__(256) fuse_kernel(V views)
 {
     __shared__ int pre[kMaxBatch + 1];
-    map_prefix(views, [](const MapView& v) { return (int)v.m.ctr[C_VISIBLE]; }, pre);
+    map_prefix(views, [](const MapView& v) { return v.in.active ? (int)v.m.ctr[C_VISIBLE] : 0; }, pre);
     const int nmaps = views.count();
     const int total = pre[nmaps];
     const int team = threadIdx.x >> 7;

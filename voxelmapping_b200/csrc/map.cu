@@ -91,6 +91,7 @@ void make_view(const vmap_map* m, const double pose[16], MapView& v)
     v.cam.cy = m->cfg.cy;
     v.cam.ifx = (float)(1.0 / (double)m->cfg.fx);
     v.cam.ify = (float)(1.0 / (double)m->cfg.fy);
+    v.in.active = 1;
     v.in.dscale = 1.f;
     if (pose) {
         double inv[16];

@@ -40,7 +40,7 @@ template <class V>
 __global__ void __launch_bounds__(256) zrange_kernel(V views)
 {
     __shared__ int pre[kMaxBatch + 1];
-    map_prefix(views, [](const MapView& v) { return v.out.mode == 0 ? allocated_blocks(v.m) : 0; }, pre);
+    map_prefix(views, [](const MapView& v) { return v.out.vmap && v.out.mode == 0 ? allocated_blocks(v.m) : 0; }, pre);
     if (blockIdx.x == 0 && threadIdx.x == 0) views.queue[0] = 0u;
     const int nmaps = views.count();
     const int total = pre[nmaps];

@@ -28,7 +28,7 @@ constexpr int kTileW = 8, kTileH = 4;
 
 __device__ __forceinline__ int ray_tiles(const MapView& v)
 {
-    return ((v.cam.W + kTileW - 1) / kTileW) * ((v.cam.H + kTileH - 1) / kTileH);
+    return v.out.vmap ? ((v.cam.W + kTileW - 1) / kTileW) * ((v.cam.H + kTileH - 1) / kTileH) : 0;
 }
 
 __device__ __forceinline__ float3 fma3(float k, float3 d, float3 r)

@@ -379,6 +379,7 @@ struct CamParams {
 };
 
 struct FrameIn {
+    int active;      // this map selects visible blocks / fuses this step
     const void* depth;
     size_t dpitch;
     int dtype;       // VMAP_DEPTH_*

@@ -228,13 +228,16 @@ class MapBatch:
             pass
 
     def step(self, depths, rgbs, poses, vmaps, nmaps=None, depth_scale=0.001, stream=None):
+        """One fuse + render step over every map of the batch. ``depths[i]`` None
+        skips map i's fusion and ``vmaps[i]`` None its render (a fuse-only or
+        render-only request); both None leave the map idle."""
         import torch
         for i, m in enumerate(self.maps):
             f = self._frames[i]
             d = depths[i]
-            f.depth_dev = d.data_ptr()
-            f.depth_type = L.DEPTH_U16 if d.dtype in (torch.uint16, torch.int16) else L.DEPTH_F32
-            f.depth_pitch = d.stride(0) * d.element_size()
+            f.depth_dev = d.data_ptr() if d is not None else None
+            f.depth_type = L.DEPTH_U16 if d is not None and d.dtype in (torch.uint16, torch.int16) else L.DEPTH_F32
+            f.depth_pitch = d.stride(0) * d.element_size() if d is not None else 0
             f.depth_scale = depth_scale
             c = rgbs[i] if rgbs is not None else None
             f.rgb_dev = c.data_ptr() if c is not None else None
@@ -242,8 +245,9 @@ class MapBatch:
             p = np.asarray(poses[i], np.float64).reshape(16)
             for k in range(16):
                 f.pose[k] = p[k]
-            f.vmap_dev = vmaps[i].data_ptr()
-            f.vmap_pitch = vmaps[i].stride(0) * 4
+            v = vmaps[i]
+            f.vmap_dev = v.data_ptr() if v is not None else None
+            f.vmap_pitch = v.stride(0) * 4 if v is not None else 0
             n = nmaps[i] if nmaps is not None else None
             f.nmap_dev = n.data_ptr() if n is not None else None
             f.nmap_pitch = n.stride(0) * 4 if n is not None else 0
