@@ -52,6 +52,7 @@ typedef enum vmap_status {
 #define VMAP_FLAG_HASH_FULL 2u
 #define VMAP_FLAG_RANGE 4u
 #define VMAP_FLAG_BUFFER_FULL 8u
+#define VMAP_FLAG_BAD_SNAPSHOT 16u /* a loaded snapshot held an invalid or repeated block key */
 
 /* Voxel storage formats. REF is the reference's Voxel (int16 TSDF x32767,
  * uint8 weight, map_struct.h:17-21); F32 is the plain single-precision map;
@@ -218,6 +219,48 @@ vmap_status vmap_copy_counters(vmap_map* map, uint32_t* dst, void* stream);
  * Buffers are host memory sized for max_blocks. Synchronous. */
 vmap_status vmap_export_blocks(vmap_map* map, int32_t* coords, float* tsdf, float* weight, uint8_t* rgb,
                                uint32_t max_blocks, uint32_t* n_blocks, void* stream);
+
+/* ---- snapshots (no counterpart in the reference; its nearest operations are
+ * reset/release, map_struct.cu:29-79). A snapshot is the map's used blocks in
+ * pool order plus their keys: enough to evict a map from the GPU (to pinned
+ * host memory) and bring it back, or to checkpoint and resume it. Loading
+ * rebuilds the hash table, so the target map may have a different number of
+ * buckets; it needs the same voxel format, colour setting, voxel size,
+ * truncation and weight cap, and capacity for the blocks. A loaded map gives
+ * bit-identical fusion, raycast and mesh results to the map it was saved from.
+ *
+ * Layout (little-endian): this 64-byte header, at keys_offset n_blocks uint64
+ * keys (block x, y, z as 21-bit two's-complement fields at bits 42, 21 and 0),
+ * at pool_offset (a multiple of 256) n_blocks blocks of block_bytes each, in the
+ * pool layout [tsdf/weight word x512][r x512][g x512][b x512] (voxel x + 8y + 64z;
+ * colour planes only with colour). */
+typedef struct vmap_snapshot_header {
+    char magic[8];          /* "VMAPSNAP"                                   */
+    uint32_t version;       /* 1                                            */
+    uint32_t header_bytes;  /* 64                                           */
+    int32_t voxel_format;
+    int32_t with_color;
+    uint32_t block_bytes;   /* vmap_block_bytes(voxel_format, with_color)   */
+    uint32_t n_blocks;
+    float voxel_size;
+    float truncation;
+    int32_t max_weight;
+    uint32_t error_flags;   /* sticky flags of the saved map                */
+    uint64_t keys_offset;
+    uint64_t pool_offset;
+} vmap_snapshot_header;
+
+/* Writes the snapshot to dst (host memory, pinned or not, or device memory).
+ * *bytes receives the snapshot size; with dst NULL nothing is written (a size
+ * query), and a capacity below the size fails with VMAP_ERR_INVALID_ARG.
+ * Synchronous: returns once dst holds the snapshot. */
+vmap_status vmap_snapshot_save(vmap_map* map, void* dst, uint64_t capacity, uint64_t* bytes, void* stream);
+/* Replaces the map's content by the snapshot at src (host or device memory,
+ * `bytes` long). Synchronous: src may be reused on return. Invalid or
+ * mismatched snapshots fail with VMAP_ERR_INVALID_ARG and leave the map as it
+ * was; a snapshot whose keys do not fit the target's hash table fails with
+ * VMAP_ERR_HASH_FULL (the map is then reset). */
+vmap_status vmap_snapshot_load(vmap_map* map, const void* src, uint64_t bytes, void* stream);
 
 /* Block export that allocates nothing. No counterpart in the reference.
  *

@@ -15,7 +15,7 @@ STATUS_NAMES = {0: "VMAP_OK", 1: "VMAP_ERR_INVALID_ARG", 2: "VMAP_ERR_CUDA", 3: 
                 4: "VMAP_ERR_POOL_FULL", 5: "VMAP_ERR_HASH_FULL", 6: "VMAP_ERR_RANGE",
                 7: "VMAP_ERR_BUFFER_FULL", 8: "VMAP_ERR_NO_DEVICE"}
 
-FLAG_POOL_FULL, FLAG_HASH_FULL, FLAG_RANGE, FLAG_BUFFER_FULL = 1, 2, 4, 8
+FLAG_POOL_FULL, FLAG_HASH_FULL, FLAG_RANGE, FLAG_BUFFER_FULL, FLAG_BAD_SNAPSHOT = 1, 2, 4, 8, 16
 
 VOXEL_REF, VOXEL_F32, VOXEL_F16, VOXEL_I16 = 0, 1, 2, 3
 FORMAT_NAMES = {"ref": VOXEL_REF, "f32": VOXEL_F32, "f16": VOXEL_F16, "i16": VOXEL_I16}
@@ -90,6 +90,8 @@ SIGNATURES = {
     "vmap_export_blocks": (C.c_int, [P, P, P, P, P, C.c_uint32, C.POINTER(C.c_uint32), P]),
     "vmap_copy_counters": (C.c_int, [P, P, P]),
     "vmap_export_blocks_static": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P, P, P, C.POINTER(C.c_uint32), P]),
+    "vmap_snapshot_save": (C.c_int, [P, P, C.c_uint64, C.POINTER(C.c_uint64), P]),
+    "vmap_snapshot_load": (C.c_int, [P, P, C.c_uint64, P]),
     "vmap_timing_enable": (C.c_int, [P, C.c_uint32]),
     "vmap_timing_read": (C.c_int, [P, C.POINTER(C.c_double), C.POINTER(C.c_uint32)]),
     "vmap_pose_inverse": (None, [DBL16, DBL16]),

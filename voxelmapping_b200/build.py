@@ -20,7 +20,7 @@ OBJ = PKG / "_build"
 LIB = PKG / "libvmap_b200.so"
 SYNTH = PKG / "libvmap_synth.so"
 
-CUDA_SOURCES = ["fusion.cu", "raycast.cu", "raymarch.cu", "mesh.cu", "map.cu", "batch.cu", "export_static.cu",
+CUDA_SOURCES = ["fusion.cu", "raycast.cu", "raymarch.cu", "mesh.cu", "map.cu", "batch.cu", "export_static.cu", "snapshot.cu",
                 "vmapping.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",

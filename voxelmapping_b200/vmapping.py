@@ -183,6 +183,32 @@ class VoxelMapping:
         k = got.value
         return {"coords": coords[:k], "tsdf": tsdf[:k], "weight": weight[:k]}
 
+    def snapshot_bytes(self):
+        """Size of vmap_snapshot_save's output for the map as it is now."""
+        n = C.c_uint64()
+        L.check(self._lib.vmap_snapshot_save(self._need(), None, 0, C.byref(n), _stream()), "vmap_snapshot_save")
+        return n.value
+
+    def save_snapshot(self, out=None):
+        """vmap_snapshot_save into `out` (a uint8 numpy array or a torch uint8
+        tensor, host, pinned or CUDA, of at least snapshot_bytes()), or into a
+        new numpy array. Returns the filled prefix."""
+        n = self.snapshot_bytes()
+        if out is None:
+            out = np.empty(n, np.uint8)
+        ptr = out.ctypes.data if isinstance(out, np.ndarray) else out.data_ptr()
+        cap = out.nbytes if isinstance(out, np.ndarray) else out.numel() * out.element_size()
+        got = C.c_uint64()
+        L.check(self._lib.vmap_snapshot_save(self._need(), C.c_void_p(ptr), cap, C.byref(got), _stream()),
+                "vmap_snapshot_save")
+        return out[:got.value]
+
+    def load_snapshot(self, snap):
+        """vmap_snapshot_load from a uint8 numpy array or torch tensor."""
+        ptr = snap.ctypes.data if isinstance(snap, np.ndarray) else snap.data_ptr()
+        nbytes = snap.nbytes if isinstance(snap, np.ndarray) else snap.numel() * snap.element_size()
+        L.check(self._lib.vmap_snapshot_load(self._need(), C.c_void_p(ptr), nbytes, _stream()), "vmap_snapshot_load")
+
     def export_blocks(self, with_rgb=None):
         """Allocated blocks in pool order: coords (n, 3) int32, tsdf / weight
         (n, 512) float32 (voxel x + 8y + 64z), rgb (n, 512, 3) uint8 or None."""
