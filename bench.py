@@ -47,6 +47,7 @@ def parse():
     p.add_argument("--batch", type=int, default=32, help="maps per batched step (0 skips the batched arm)")
     p.add_argument("--batch-steps", type=int, default=0, help="timed batched steps (default: --steps // 4)")
     p.add_argument("--batch-blocks", type=int, default=1 << 17, help="block pool per batched map")
+    p.add_argument("--uneven", type=int, default=64, help="maps of the uneven batch (0 skips it)")
     return p.parse_args()
 
 
@@ -181,56 +182,57 @@ def run_reference(args):
 
 
 # -------------------------------------------------------------- batched arm
-def run_batched(args, wl, dev, flush, world, plain_value):
-    """B maps of the same 640x480 / 5 mm workload, FP16 TSDF + uint16 weight +
-    colour, each fed its own seeded scene; one vmap_batch_step per step (one
-    launch per stage over all maps, graph-replayed on a side stream)."""
-    import dataclasses
-
+def run_batched(args, wls, dev, flush, world, plain_value, distinct_frames=None):
+    """One map per workload in `wls` (one voxel format for all), each fed its
+    own seeded scene; one vmap_batch_step per step (one launch per stage over
+    all maps, graph-replayed on a side stream). With `distinct_frames` F, each
+    map renders F frames and the steps cycle through them."""
     import torch
     import torch.distributed as dist
     from voxelmapping_b200 import MapBatch, VoxelMapping
     from voxelmapping_b200 import _lib as L
     from voxelmapping_b200 import synth
 
-    rank = int(os.environ.get("RANK", 0))
-    B = args.batch
+    B = len(wls)
     K = args.batch_steps or max(4, args.steps // 4)
     W = min(args.warmup, 5)
     nfr = W + K
-    wlb = dataclasses.replace(wl, voxel_format="f16", max_weight=128, num_blocks=args.batch_blocks)
-    H, Wd = wlb.height, wlb.width
-    depth = torch.empty((B, nfr, H, Wd), dtype=torch.int16, device=dev)
-    rgb = torch.empty((B, nfr, H, Wd * 3), dtype=torch.uint8, device=dev)
-    poses = np.zeros((B, nfr, 16))
-    for b in range(B):
-        sc = synth.Scene(dataclasses.replace(wlb, seed=1000 * (rank + 1) + b))
-        for i in range(nfr):
-            d, c, p = sc.render(i)
-            depth[b, i].copy_(torch.from_numpy(d.view(np.int16)))
-            rgb[b, i].copy_(torch.from_numpy(c).reshape(H, Wd * 3))
-            poses[b, i] = p.reshape(16)
+    F = min(nfr, distinct_frames or nfr)
+    maps, depth, rgb, poses, vmaps, nmaps = [], [], [], [], [], []
+    for b, w in enumerate(wls):
+        sc = synth.Scene(w)
+        d_b = torch.empty((F, w.height, w.width), dtype=torch.int16, device=dev)
+        c_b = torch.empty((F, w.height, w.width * 3), dtype=torch.uint8, device=dev) if w.with_color else None
+        p_b = np.zeros((F, 16))
+        stride = max(1, w.n_poses // max(F, 1)) if F < nfr else 1
+        for i in range(F):
+            d, c, p = sc.render(i * stride)
+            d_b[i].copy_(torch.from_numpy(d.view(np.int16)))
+            if c_b is not None:
+                c_b[i].copy_(torch.from_numpy(c).reshape(w.height, -1))
+            p_b[i] = p.reshape(16)
         del sc
-    maps = []
-    for b in range(B):
-        vm = VoxelMapping(Wd, H, wlb.K, voxel_format="f16", with_color=True, max_weight=128)
-        vm.CreateMap(wlb.num_entries, wlb.num_blocks, wlb.voxel_size)
+        depth.append(d_b), rgb.append(c_b), poses.append(p_b)
+        vmaps.append(torch.empty((w.height, w.width, 4), dtype=torch.float32, device=dev))
+        nmaps.append(torch.empty((w.height, w.width, 4), dtype=torch.float32, device=dev))
+        vm = VoxelMapping(w.width, w.height, w.K, voxel_format=w.voxel_format, with_color=w.with_color,
+                          max_weight=w.max_weight)
+        vm.CreateMap(w.num_entries, w.num_blocks, w.voxel_size)
         maps.append(vm)
     batch = MapBatch(maps)
-    vmaps = torch.empty((B, H, Wd, 4), dtype=torch.float32, device=dev)
-    nmaps = torch.empty_like(vmaps)
     frames = []
     for i in range(nfr):
         fr = (L.BatchFrame * B)()
-        for b in range(B):
-            f = fr[b]
-            f.depth_dev, f.depth_type, f.depth_pitch, f.depth_scale = depth[b, i].data_ptr(), L.DEPTH_U16, Wd * 2, \
-                wlb.depth_scale
-            f.rgb_dev, f.rgb_pitch = rgb[b, i].data_ptr(), Wd * 3
+        for b, w in enumerate(wls):
+            f, j = fr[b], i % F
+            f.depth_dev, f.depth_type, f.depth_pitch, f.depth_scale = depth[b][j].data_ptr(), L.DEPTH_U16, \
+                w.width * 2, w.depth_scale
+            if rgb[b] is not None:
+                f.rgb_dev, f.rgb_pitch = rgb[b][j].data_ptr(), w.width * 3
             for k in range(16):
-                f.pose[k] = poses[b, i, k]
-            f.vmap_dev, f.vmap_pitch = vmaps[b].data_ptr(), Wd * 16
-            f.nmap_dev, f.nmap_pitch = nmaps[b].data_ptr(), Wd * 16
+                f.pose[k] = poses[b][j, k]
+            f.vmap_dev, f.vmap_pitch = vmaps[b].data_ptr(), w.width * 16
+            f.nmap_dev, f.nmap_pitch = nmaps[b].data_ptr(), w.width * 16
         frames.append(fr)
     lib = L.lib()
     side = torch.cuda.Stream(device=dev)
@@ -254,19 +256,43 @@ def run_batched(args, wl, dev, flush, world, plain_value):
     if world > 1:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
     value = world * B * K / (float(t.item()) / 1e3)
-    hits = float(torch.isfinite(vmaps[:, :, :, 0]).float().mean().item())
-    flags = [m.stats()["error_flags"] for m in maps]
+    pixels = sum(w.width * w.height for w in wls)
+    hits = float(sum(torch.isfinite(v[..., 0]).sum().item() for v in vmaps)) / pixels
+    stats = [m.stats() for m in maps]
     batch.release()
     for m in maps:
         m.release()
     return {"value": value, "unit": "frames/s", "maps": B, "steps": K, "warmup": W,
             "ms_per_step": float(t.item()) / K, "p50_ms_per_step": percentile(step_ms, 50),
             "p99_ms_per_step": percentile(step_ms, 99), "ratio_vs_plain": value / plain_value,
-            "dtype": "f16", "hit_fraction_last_step": hits, "error_flags": int(max(flags)),
-            "config": "%d maps x 640x480 depth + rgb, 5 mm voxels, FP16 TSDF + uint16 weight (cap 128) + uint8x3 "
-                      "colour, 2^%d-block pool each, each map its own seeded room scene and figure-8; one step = "
-                      "one frame per map fused + raycast (vmap_batch_step: one launch per stage over all maps, "
-                      "CUDA-graph replay); L2 flushed between steps" % (B, int(np.log2(wlb.num_blocks)))}
+            "megapixels_per_step": pixels / 1e6, "dtype": wls[0].voxel_format,
+            "hit_fraction_last_step": hits, "error_flags": int(np.bitwise_or.reduce([s["error_flags"] for s in stats])),
+            "allocated_blocks_total": int(sum(s["allocated_blocks"] for s in stats))}
+
+
+def batched_same_size(args, wl, rank):
+    """args.batch maps of the 640x480 / 5 mm workload, FP16 TSDF + uint16
+    weight (cap 128) + colour, each its own seeded room and figure-8."""
+    import dataclasses
+    wlb = dataclasses.replace(wl, voxel_format="f16", max_weight=128, num_blocks=args.batch_blocks)
+    wls = [dataclasses.replace(wlb, seed=1000 * (rank + 1) + b) for b in range(args.batch)]
+    desc = ("%d maps x 640x480 depth + rgb, 5 mm voxels, FP16 TSDF + uint16 weight (cap 128) + uint8x3 colour, "
+            "2^%d-block pool each, each map its own seeded room scene and figure-8; one step = one frame per map "
+            "fused + raycast (vmap_batch_step: one launch per stage over all maps, CUDA-graph replay); L2 flushed "
+            "between steps" % (args.batch, int(np.log2(wlb.num_blocks))))
+    return wls, desc
+
+
+def batched_uneven(args, rank):
+    """args.uneven maps of uneven extent U(1,8) m, voxel size {4,8,12,16} mm,
+    resolution {320x240, 640x480, 1280x720}, pools 2^14..2^19, FP16 + colour."""
+    from voxelmapping_b200 import synth
+    wls = synth.uneven_workloads(args.uneven, seed=rank + 1)
+    desc = ("%d maps of uneven extent U(1,8) m, voxel size {4,8,12,16} mm, depth resolution {320x240, 640x480, "
+            "1280x720}, pools 2^14..2^19 blocks, FP16 TSDF + uint16 weight (cap 128) + uint8x3 colour, each its own "
+            "seeded scene; one step = one frame per map fused + raycast in one vmap_batch_step; each map cycles "
+            "through 8 rendered frames; L2 flushed between steps" % args.uneven)
+    return wls, desc
 
 
 # --------------------------------------------------------------- product arm
@@ -426,9 +452,16 @@ def run_product(args):
                        "path": "vmap_fuse_host + vmap_render_scene_host, pinned host buffers"}
 
     # --- batched arm: many maps per step ------------------------------------
-    if args.batch > 0:
+    if args.batch > 0 or args.uneven > 0:
         vm.release()
-        line["batched"] = run_batched(args, wl, dev, flush, world, value)
+    if args.batch > 0:
+        wls, desc = batched_same_size(args, wl, rank)
+        line["batched"] = run_batched(args, wls, dev, flush, world, value)
+        line["batched"]["config"] = desc
+    if args.uneven > 0:
+        wls, desc = batched_uneven(args, rank)
+        line["batched_uneven"] = run_batched(args, wls, dev, flush, world, value, distinct_frames=8)
+        line["batched_uneven"]["config"] = desc
 
     # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

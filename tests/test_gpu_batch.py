@@ -139,3 +139,47 @@ def test_batch_fuse_only_and_render_only_frames():
             assert np.array_equal(ea[k][ia], eb[k][ib]), k
         assert a.stats()["error_flags"] == 0
     batch.release()
+
+
+def test_uneven_batch_equals_single_map_calls():
+    """Maps of uneven extent, voxel size (4-16 mm), resolution (up to
+    1280x720) and pool size in one batch."""
+    # pools 4x the generator's so no allocation is refused (which blocks a full
+    # pool refuses depends on scheduling order)
+    wls = [dataclasses.replace(w, num_blocks=4 * w.num_blocks) for w in synth.uneven_workloads(10, seed=3)]
+    assert len({(w.width, w.voxel_size, w.num_blocks) for w in wls}) >= 6
+    scenes = [synth.Scene(wl) for wl in wls]
+    mk = lambda wl: VoxelMapping(wl.width, wl.height, wl.K, voxel_format=wl.voxel_format, with_color=wl.with_color,
+                                 max_weight=wl.max_weight)
+    batch_maps, solo_maps = [mk(wl) for wl in wls], [mk(wl) for wl in wls]
+    for m, wl in zip(batch_maps + solo_maps, wls + wls):
+        m.CreateMap(wl.num_entries, wl.num_blocks, wl.voxel_size)
+    batch = MapBatch(batch_maps)
+    side = torch.cuda.Stream()
+    for step in range(3):
+        frames = [sc.render(step * 7) for sc in scenes]
+        depths = [torch.from_numpy(d.view(np.int16)).cuda() for d, _, _ in frames]
+        rgbs = [torch.from_numpy(c).cuda().reshape(wl.height, -1) for (_, c, _), wl in zip(frames, wls)]
+        poses = [p for _, _, p in frames]
+        vb = [torch.full((wl.height, wl.width, 4), 7.0, device="cuda") for wl in wls]
+        nb = [torch.full((wl.height, wl.width, 4), 7.0, device="cuda") for wl in wls]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            batch.step(depths, rgbs, poses, vb, nb)
+        side.synchronize()
+        for i, vm in enumerate(solo_maps):
+            vm.FuseDepthAndImage(rgbs[i], depths[i], poses[i])
+            nm = torch.empty_like(vb[i])
+            v = vm.RenderScene(None, poses[i], nmap=nm)
+            torch.cuda.synchronize()
+            assert np.array_equal(np.nan_to_num(v.cpu().numpy(), nan=-9.0), np.nan_to_num(vb[i].cpu().numpy(), nan=-9.0)), (step, i)
+            assert np.array_equal(np.nan_to_num(nm.cpu().numpy(), nan=-9.0), np.nan_to_num(nb[i].cpu().numpy(), nan=-9.0)), (step, i)
+    hit = np.mean([np.isfinite(v.cpu().numpy()[..., 0]).mean() for v in vb])
+    assert hit > 0.3
+    for a, b in zip(batch_maps, solo_maps):
+        ea, eb = a.export_blocks(), b.export_blocks()
+        ia, ib = np.argsort(block_keys(ea["coords"])), np.argsort(block_keys(eb["coords"]))
+        for k in ("coords", "tsdf", "weight", "rgb"):
+            assert np.array_equal(ea[k][ia], eb[k][ib]), k
+        assert a.stats()["error_flags"] == b.stats()["error_flags"] == 0
+    batch.release()

@@ -151,6 +151,11 @@ vmap_status vmap_snapshot_save(vmap_map* map, void* dst, uint64_t capacity, uint
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     unsigned char* d = static_cast<unsigned char*>(dst);
     SNAP_CK(cudaMemcpyAsync(d, &h, sizeof(h), cudaMemcpyDefault, s));
+    // zero the padding before the aligned pool so equal maps give equal bytes
+    static const unsigned char zeros[kPoolAlign] = {};
+    const uint64_t keys_end = h.keys_offset + 8ull * n;
+    if (h.pool_offset > keys_end)
+        SNAP_CK(cudaMemcpyAsync(d + keys_end, zeros, h.pool_offset - keys_end, cudaMemcpyDefault, s));
     if (n) {
         SNAP_CK(cudaMemcpyAsync(d + h.keys_offset, m.blockKeys, 8ull * n, cudaMemcpyDefault, s));
         SNAP_CK(cudaMemcpyAsync(d + h.pool_offset, m.pool, (size_t)n * h.block_bytes, cudaMemcpyDefault, s));

@@ -8,6 +8,7 @@ Workloads (seeded, no external data):
   room_full  : 640x480, f 525, c (319.5, 239.5), 500 poses on a figure-8;
                5 mm voxels, 2^21 entries, 2^20 blocks; FP32 TSDF + float
                weight + uint8x3 colour.
+  uneven_workloads(n): n maps of uneven extent, voxel size and resolution.
 Scene: 4 x 4 x 3 m box room seen from inside + 8 spheres, radius U(0.1, 0.5) m;
 depth uint16 mm with N(0, 0.0012 + 0.0019 (z - 0.4)^2) m noise and 2 % dropouts.
 """
@@ -90,6 +91,36 @@ WORKLOADS = {
     "room_full": Workload("room_full", 640, 480, 525.0, 525.0, 319.5, 239.5, 500, TRAJ_FIGURE8, 0.005,
                           1 << 21, 1 << 20, "f32", True),
 }
+
+
+RESOLUTIONS = ((320, 240), (640, 480), (1280, 720))
+VOXEL_SIZES = (0.004, 0.008, 0.012, 0.016)
+
+
+def uneven_workloads(n, seed=0, voxel_format="f16", with_color=True):
+    """n independent map workloads of uneven size (the batching / serving mix):
+    room extent U(1, 8) m, voxel size from {4, 8, 12, 16} mm, depth resolution
+    from {320x240, 640x480, 1280x720} (focal length 0.82 x width, principal
+    point at the centre), each its own seeded scene and trajectory. The pool
+    is the power of two (clamped to 2^14 .. 2^19 blocks) above 1.5x the
+    room's surface area in block faces."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        e = float(rng.uniform(1.0, 8.0))
+        room = (e, e * float(rng.uniform(0.6, 1.0)), min(3.0, max(1.0, 0.6 * e)))
+        vs = float(VOXEL_SIZES[rng.integers(len(VOXEL_SIZES))])
+        w, h = RESOLUTIONS[rng.integers(len(RESOLUTIONS))]
+        f = 0.8203125 * w
+        area = 2.0 * (room[0] * room[1] + room[0] * room[2] + room[1] * room[2])
+        est = 1.5 * area / (8 * vs) ** 2
+        blocks = 1 << int(min(19, max(14, int(np.ceil(np.log2(est))))))
+        out.append(Workload("uneven%d" % i, w, h, f, f, (w - 1) / 2.0, (h - 1) / 2.0, 100,
+                            TRAJ_FIGURE8 if i % 2 else TRAJ_CIRCLE, vs, 4 * blocks, blocks, voxel_format,
+                            with_color, max_weight=128, room=room,
+                            cam_radius=0.25 * min(room[0], room[1]), cam_height=0.5 * room[2],
+                            seed=int(seed) * 100003 + 17 + i))
+    return out
 
 
 class Scene:
