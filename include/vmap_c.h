@@ -104,6 +104,18 @@ typedef struct vmap_map vmap_map;
  * allocates the hash table, block pool and work buffers on the current device
  * and resets them. Synchronous. */
 vmap_status vmap_create(const vmap_config* cfg, vmap_map** out);
+/* Maps in caller-owned device memory (no counterpart in the reference): a
+ * server that keeps many maps resident and swaps them in and out places them
+ * in memory it manages, so creating and destroying a map allocates and frees
+ * no device memory. vmap_required_bytes gives the size for a configuration;
+ * vmap_create_in builds the map inside device_mem (256-byte aligned, at
+ * least that many bytes) and resets it asynchronously on `stream`. The
+ * memory must stay valid until vmap_destroy, which then frees only what the
+ * map allocated itself (host-call staging, mesh buffers) and does not
+ * synchronise the device: the caller first finishes the work on the map. */
+vmap_status vmap_required_bytes(const vmap_config* cfg, uint64_t* bytes);
+vmap_status vmap_create_in(const vmap_config* cfg, void* device_mem, uint64_t bytes, void* stream,
+                           vmap_map** out);
 /* ~VoxelMapping / MapStruct::release (map_struct.cu:68-79). Synchronous. */
 vmap_status vmap_destroy(vmap_map* map);
 /* VoxelMapping::reset / MapStruct::reset (map_struct.cu:29-42): empties the
@@ -156,7 +168,9 @@ vmap_status vmap_render_phong(const float* vmap_dev, size_t vmap_pitch, const fl
 /* Polygonize (marching_cubes.cu:251-305): marching cubes over all allocated
  * blocks. Writes at most max_tris triangles (9 floats each for verts and
  * norms, world metres); the unclamped count goes to *n_tris_dev (device
- * uint32, may be NULL) and to vmap_stats.last_triangles. */
+ * uint32, may be NULL) and to vmap_stats.last_triangles. With verts_dev NULL
+ * the call only counts; otherwise a count above max_tris sets
+ * VMAP_FLAG_BUFFER_FULL. */
 vmap_status vmap_polygonize(vmap_map* map, float* verts_dev, float* norms_dev, uint32_t max_tris,
                             uint32_t* n_tris_dev, void* stream);
 /* VoxelMapping::Polygonize (vmapping.cpp:119-132, 182): mesh into library-owned
@@ -199,6 +213,14 @@ typedef struct vmap_batch_frame {
 
 #define VMAP_MAX_BATCH 256
 vmap_status vmap_batch_create(vmap_map* const* maps, int n_maps, vmap_batch** out);
+/* A batch of n_slots empty slots for maps of one voxel format. Slots are
+ * filled and emptied between steps with vmap_batch_set_map (NULL empties a
+ * slot); the recorded graphs stay valid, so a server can swap maps in and
+ * out of a long-lived batch. An empty slot's frame must have all pointers
+ * NULL. Calling vmap_batch_set_map on a batch made by vmap_batch_create
+ * synchronises the device once and records its graphs again. */
+vmap_status vmap_batch_create_slots(int n_slots, int voxel_format, vmap_batch** out);
+vmap_status vmap_batch_set_map(vmap_batch* batch, int slot, vmap_map* map);
 vmap_status vmap_batch_destroy(vmap_batch* batch);
 /* frames: n_maps entries. Asynchronous on `stream`; may block only until the
  * step before last has copied its descriptors. */

@@ -183,3 +183,93 @@ def test_uneven_batch_equals_single_map_calls():
             assert np.array_equal(ea[k][ia], eb[k][ib]), k
         assert a.stats()["error_flags"] == b.stats()["error_flags"] == 0
     batch.release()
+
+
+def test_slot_batch_with_maps_in_caller_memory():
+    """vmap_batch_create_slots + vmap_batch_set_map with maps built by
+    vmap_create_in: maps move between slots and sit out steps (empty slot)
+    while the recorded graphs are replayed; results equal single-map calls."""
+    import ctypes as C
+    lib = L.lib()
+    wls = workloads()
+    scenes = [synth.Scene(wl) for wl in wls]
+    solo_maps = [make_map(wl) for wl in wls]
+    slot_maps, mems = [], []
+    for wl in wls:
+        vm = VoxelMapping(wl.width, wl.height, wl.K, voxel_format=wl.voxel_format, with_color=wl.with_color,
+                          max_weight=128)
+        need = vm.required_bytes(1 << 18, wl.num_blocks, wl.voxel_size)
+        mem = torch.full((need + 4096,), 0xAB, dtype=torch.uint8, device="cuda")  # dirty memory
+        vm.CreateMapIn(1 << 18, wl.num_blocks, wl.voxel_size, mem)
+        assert vm.stats()["device_bytes"] == need
+        slot_maps.append(vm)
+    with pytest.raises(L.VmapError):
+        VoxelMapping(wls[0].width, wls[0].height, wls[0].K, voxel_format="f16").CreateMapIn(
+            1 << 18, wls[0].num_blocks, wls[0].voxel_size, torch.empty(1000, dtype=torch.uint8, device="cuda"))
+    h = C.c_void_p()
+    L.check(lib.vmap_batch_create_slots(5, L.VOXEL_F16, C.byref(h)))
+    f32 = VoxelMapping(64, 48, wls[0].K, voxel_format="f32")
+    f32.CreateMap(1 << 10, 1 << 10, 0.01)
+    assert lib.vmap_batch_set_map(h, 0, f32._map) == 1
+    side = torch.cuda.Stream()
+    # slot of each map per step (None: not in the batch this step)
+    layout = [[0, 1, 2], [4, 1, 2], [4, None, 0], [3, 1, 0], [3, 2, 1], [0, 2, 1]]
+    cur = [None] * 3
+    frames = (L.BatchFrame * 5)()
+    for step, slots in enumerate(layout):
+        for i, sl in enumerate(slots):  # empty old slots first, then fill
+            if cur[i] is not None and cur[i] != sl:
+                L.check(lib.vmap_batch_set_map(h, cur[i], None))
+        for i, sl in enumerate(slots):
+            if sl is not None:
+                L.check(lib.vmap_batch_set_map(h, sl, slot_maps[i]._map))
+            cur[i] = sl
+        for k in range(5):
+            fr = frames[k]
+            fr.depth_dev = fr.rgb_dev = fr.vmap_dev = fr.nmap_dev = None
+        keep, outs = [], {}
+        for i, (wl, sc) in enumerate(zip(wls, scenes)):
+            if slots[i] is None:
+                continue
+            d, c, p = sc.render(step * 3)
+            dt = torch.from_numpy(d.view(np.int16)).cuda()
+            ct = torch.from_numpy(c).cuda().reshape(wl.height, -1) if wl.with_color else None
+            vb = torch.full((wl.height, wl.width, 4), 7.0, device="cuda")
+            nb = torch.full((wl.height, wl.width, 4), 7.0, device="cuda")
+            keep += [dt, ct, vb, nb]
+            fr = frames[slots[i]]
+            fr.depth_dev, fr.depth_type, fr.depth_pitch, fr.depth_scale = dt.data_ptr(), L.DEPTH_U16, wl.width * 2, 0.001
+            if ct is not None:
+                fr.rgb_dev, fr.rgb_pitch = ct.data_ptr(), wl.width * 3
+            fr.pose[:] = [float(x) for x in p.reshape(16)]
+            fr.vmap_dev, fr.vmap_pitch, fr.nmap_dev, fr.nmap_pitch = vb.data_ptr(), wl.width * 16, nb.data_ptr(), \
+                wl.width * 16
+            outs[i] = (dt, ct, p, vb, nb)
+        torch.cuda.synchronize()
+        L.check(lib.vmap_batch_step(h, frames, C.c_void_p(side.cuda_stream)))
+        side.synchronize()
+        for i, (dt, ct, p, vb, nb) in outs.items():
+            vm = solo_maps[i]
+            if ct is not None:
+                vm.FuseDepthAndImage(ct, dt, p)
+            else:
+                vm.FuseDepth(dt, p)
+            nm = torch.empty_like(vb)
+            v = vm.RenderScene(None, p, nmap=nm)
+            torch.cuda.synchronize()
+            assert np.array_equal(np.nan_to_num(v.cpu().numpy(), nan=-9.0), np.nan_to_num(vb.cpu().numpy(), nan=-9.0)), (step, i)
+            assert np.array_equal(np.nan_to_num(nm.cpu().numpy(), nan=-9.0), np.nan_to_num(nb.cpu().numpy(), nan=-9.0)), (step, i)
+    # a frame for an empty slot is refused
+    for k in range(5):
+        frames[k].depth_dev = frames[k].rgb_dev = frames[k].vmap_dev = frames[k].nmap_dev = None
+    frames[4].vmap_dev = keep[2].data_ptr()
+    assert lib.vmap_batch_step(h, frames, C.c_void_p(side.cuda_stream)) == 1
+    side.synchronize()
+    for wl, a, b in zip(wls, slot_maps, solo_maps):
+        ea, eb = a.export_blocks(), b.export_blocks()
+        ia, ib = np.argsort(block_keys(ea["coords"])), np.argsort(block_keys(eb["coords"]))
+        for k in ("coords", "tsdf", "weight") + (("rgb",) if wl.with_color else ()):
+            assert np.array_equal(ea[k][ia], eb[k][ib]), k
+    L.check(lib.vmap_batch_destroy(h))
+    for vm in slot_maps:
+        vm.release()

@@ -273,6 +273,9 @@ def test_mesh_buffer_full_flag(small_scene):
     d, _, pose = small_scene.render(0)
     fuse_both(vm, om, d, None, pose)
     cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    # a counting pass (no buffers) flags nothing
+    L.check(L.lib().vmap_polygonize(vm._map, None, None, 0, cnt.data_ptr(), torch.cuda.current_stream().cuda_stream))
+    assert vm.stats()["error_flags"] == 0 and int(cnt.item()) > 100
     verts = torch.empty((100, 9), dtype=torch.float32, device="cuda")
     norms = torch.empty((100, 9), dtype=torch.float32, device="cuda")
     L.check(L.lib().vmap_polygonize(vm._map, verts.data_ptr(), norms.data_ptr(), 100, cnt.data_ptr(),

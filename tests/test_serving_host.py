@@ -1,0 +1,121 @@
+"""Serving scheduler (voxelmapping_b200.serving.Scheduler) on the host with a
+fake executor: every request completes, requests of a session complete in
+arrival order, a session is only served while resident, resident bytes never
+exceed the budget, eviction picks idle sessions, and oversize sessions are
+refused up front."""
+import numpy as np
+import pytest
+
+from voxelmapping_b200 import serving as S
+
+
+class FakeExecutor:
+    def __init__(self, sched):
+        self.sched = sched
+        self.resident = set()
+        self.log = []
+        self.t = 0.0
+
+    def run_tick(self, plan, clock):
+        for s in plan.evict:
+            assert s in self.resident
+            self.resident.remove(s)
+        for s in plan.restore:
+            assert s not in self.resident
+            self.resident.add(s)
+        assert sum(self.sched.bytes[s] for s in self.resident) <= self.sched.budget
+        assert len(self.resident) <= self.sched.max_resident
+        touched = [s for s, _, _ in plan.batch] + [r.session for r in plan.mesh]
+        assert len(touched) == len(set(touched)), "one request group per session per tick"
+        assert len(plan.mesh) <= self.sched.max_mesh
+        for s in touched:
+            assert s in self.resident
+        assert not (set(plan.evict) & set(touched))
+        for s, f, r in plan.batch:
+            assert f is not None or r is not None
+            if f is not None:
+                assert f.kind == "fuse" and f.session == s
+            if r is not None:
+                assert r.kind == "raycast" and r.session == s
+        self.t += 1e-4
+        for r in plan.requests():
+            r.done = clock()
+            self.log.append(r)
+
+
+def run(n_sessions, rate, count, budget_frac, seed=0, max_resident=S.MAX_RESIDENT):
+    rng = np.random.default_rng(seed)
+    sizes = [int(x) for x in rng.integers(1, 20, n_sessions) * 1000]
+    budget = max(max(sizes), int(sum(sizes) * budget_frac))
+    sched = S.Scheduler(sizes, budget, max_mesh_per_tick=2, max_resident=max_resident)
+    ex = FakeExecutor(sched)
+    reqs = S.poisson_requests(n_sessions, rate, count, seed=seed)
+    out, stats = S.serve(reqs, sched, ex, clock=lambda: ex.t, wait_until=lambda t: setattr(ex, "t", max(ex.t, t)))
+    return out, stats, ex
+
+
+@pytest.mark.parametrize("budget_frac,max_resident", [(1.0, 256), (0.3, 256), (0.05, 256), (1.0, 4)])
+def test_every_request_completes_in_session_order(budget_frac, max_resident):
+    out, stats, ex = run(40, 1e9, 3000, budget_frac, max_resident=max_resident)
+    assert all(np.isfinite(r.done) for r in out)
+    assert len(ex.log) == len(out) == 3000
+    by_session = {}
+    for r in sorted(out, key=lambda r: (r.tick, r.index)):
+        by_session.setdefault(r.session, []).append(r.index)
+    for s, idx in by_session.items():
+        assert idx == sorted(idx), s
+    if budget_frac < 1.0 or max_resident < 40:
+        assert stats["evictions"] > 0
+    else:
+        assert stats["evictions"] == 0 and stats["restores"] == 40
+
+
+def test_fuse_then_raycast_share_a_batch_frame():
+    sched = S.Scheduler([10, 10], 100)
+    reqs = [S.Request("fuse", 0, 0.0, 0), S.Request("raycast", 0, 0.1, 1), S.Request("raycast", 1, 0.2, 2),
+            S.Request("fuse", 1, 0.3, 3), S.Request("mesh", 0, 0.4, 4)]
+    for r in reqs:
+        sched.submit(r)
+    p = sched.plan()
+    assert [(s, f and f.index, r and r.index) for s, f, r in p.batch] == [(0, 0, 1), (1, None, 2)]
+    assert p.restore == [0, 1] and not p.mesh
+    p = sched.plan()
+    assert [(s, f and f.index, r and r.index) for s, f, r in p.batch] == [(1, 3, None)]
+    assert [r.index for r in p.mesh] == [4]
+    assert sched.waiting == 0 and not sched.plan().requests()
+
+
+def test_eviction_takes_least_recently_used_idle_sessions():
+    sched = S.Scheduler([10, 10, 10, 10], 30)
+    for i, s in enumerate([0, 1, 2]):
+        sched.submit(S.Request("fuse", s, float(i), i))
+    p = sched.plan()
+    assert p.restore == [0, 1, 2] and not p.evict
+    sched.submit(S.Request("fuse", 1, 5.0, 10))
+    sched.plan()  # session 1 becomes most recently used
+    sched.submit(S.Request("fuse", 3, 6.0, 11))
+    p = sched.plan()
+    assert p.evict == [0] and p.restore == [3]
+    # a session that cannot fit while all others are busy waits
+    sched2 = S.Scheduler([20, 20], 30)
+    sched2.submit(S.Request("fuse", 0, 0.0, 0))
+    sched2.submit(S.Request("fuse", 1, 0.0, 1))
+    p = sched2.plan()
+    assert p.restore == [0] and sched2.waiting == 1
+    p = sched2.plan()
+    assert p.evict == [0] and p.restore == [1]
+
+
+def test_oversize_session_is_refused():
+    with pytest.raises(ValueError):
+        S.Scheduler([10, 50], 40)
+
+
+def test_poisson_mix_and_rate():
+    reqs = S.poisson_requests(256, 1000.0, 20000, seed=3)
+    kinds = np.array([S.KINDS.index(r.kind) for r in reqs])
+    frac = np.bincount(kinds, minlength=3) / len(reqs)
+    assert np.allclose(frac, [0.70, 0.25, 0.05], atol=0.015)
+    gaps = np.diff([r.arrival for r in reqs])
+    assert abs(gaps.mean() - 1e-3) < 5e-5 and gaps.min() >= 0
+    assert len({r.session for r in reqs}) == 256

@@ -90,6 +90,10 @@ SIGNATURES = {
     "vmap_export_blocks": (C.c_int, [P, P, P, P, P, C.c_uint32, C.POINTER(C.c_uint32), P]),
     "vmap_copy_counters": (C.c_int, [P, P, P]),
     "vmap_export_blocks_static": (C.c_int, [P, C.c_uint32, C.c_uint32, P, P, P, P, C.POINTER(C.c_uint32), P]),
+    "vmap_required_bytes": (C.c_int, [C.POINTER(Config), C.POINTER(C.c_uint64)]),
+    "vmap_create_in": (C.c_int, [C.POINTER(Config), P, C.c_uint64, P, C.POINTER(P)]),
+    "vmap_batch_create_slots": (C.c_int, [C.c_int, C.c_int, C.POINTER(P)]),
+    "vmap_batch_set_map": (C.c_int, [P, C.c_int, P]),
     "vmap_snapshot_save": (C.c_int, [P, P, C.c_uint64, C.POINTER(C.c_uint64), P]),
     "vmap_snapshot_load": (C.c_int, [P, P, C.c_uint64, P]),
     "vmap_timing_enable": (C.c_int, [P, C.c_uint32]),

@@ -67,6 +67,34 @@ void release(vmap_batch* b)
     cudaFree(b->dQueue);
 }
 
+// Work-item count that makes the alloc and normals launches use their full
+// grid (their kernels stride over the items of every map, so any grid is
+// correct): slot batches change maps between steps without new graphs.
+constexpr int kFullGrid = 1 << 30;
+
+vmap_status finish_create(vmap_batch* b, vmap_batch** out)
+{
+    int dev = 0, sms = 1;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    b->launcher.numSMs = sms;
+    const size_t bytes = sizeof(MapView) * b->maps.size();
+    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
+        e = cudaMalloc((void**)&b->dViews[i], bytes);
+        if (e == cudaSuccess) e = cudaHostAlloc((void**)&b->hViews[i], bytes, cudaHostAllocDefault);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->copied[i], cudaEventDisableTiming);
+    }
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->dQueue, sizeof(unsigned));
+    if (e != cudaSuccess) {
+        vmap_status st = fail(e, "vmap_batch_create");
+        release(b);
+        delete b;
+        return st;
+    }
+    *out = b;
+    return VMAP_OK;
+}
+
 // The six stage launches of one step over the descriptors in dViews[buf].
 cudaError_t enqueue_stages(vmap_batch* b, int buf, cudaStream_t s)
 {
@@ -110,24 +138,49 @@ vmap_status vmap_batch_create(vmap_map* const* maps, int n_maps, vmap_batch** ou
         b->totalAllocTiles += tiles_32x8(c.width, c.height);
     }
     b->totalNormalTiles = b->totalAllocTiles;
-    int dev = 0, sms = 1;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    b->launcher.numSMs = sms;
-    const size_t bytes = sizeof(MapView) * (size_t)n_maps;
-    for (int i = 0; i < 2 && e == cudaSuccess; ++i) {
-        e = cudaMalloc((void**)&b->dViews[i], bytes);
-        if (e == cudaSuccess) e = cudaHostAlloc((void**)&b->hViews[i], bytes, cudaHostAllocDefault);
-        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->copied[i], cudaEventDisableTiming);
+    return finish_create(b, out);
+}
+
+vmap_status vmap_batch_create_slots(int n_slots, int voxel_format, vmap_batch** out)
+{
+    if (!out || n_slots < 1 || n_slots > kMaxBatch || vmap_block_bytes(voxel_format, 0) == 0)
+        return VMAP_ERR_INVALID_ARG;
+    *out = nullptr;
+    vmap_batch* b = new (std::nothrow) vmap_batch();
+    if (!b) return VMAP_ERR_OUT_OF_MEMORY;
+    b->fmt = voxel_format;
+    b->maps.assign(n_slots, nullptr);
+    b->totalAllocTiles = b->totalNormalTiles = kFullGrid;
+    return finish_create(b, out);
+}
+
+vmap_status vmap_batch_set_map(vmap_batch* b, int slot, vmap_map* map)
+{
+    if (!b || slot < 0 || slot >= (int)b->maps.size()) return VMAP_ERR_INVALID_ARG;
+    if (map) {
+        vmap_config c;
+        if (vmap_get_config(map, &c) != VMAP_OK || c.voxel_format != b->fmt) {
+            set_last_error("vmap_batch_set_map: the map's voxel format differs from the batch's");
+            return VMAP_ERR_INVALID_ARG;
+        }
+        for (int j = 0; j < (int)b->maps.size(); ++j)
+            if (j != slot && b->maps[j] == map) {
+                set_last_error("vmap_batch_set_map: the map is already in slot " + std::to_string(j));
+                return VMAP_ERR_INVALID_ARG;
+            }
     }
-    if (e == cudaSuccess) e = cudaMalloc((void**)&b->dQueue, sizeof(unsigned));
-    if (e != cudaSuccess) {
-        vmap_status st = fail(e, "vmap_batch_create");
-        release(b);
-        delete b;
-        return st;
+    if (b->totalAllocTiles != kFullGrid) {
+        // grids were sized for the original maps: from now on launch full
+        // grids, and record the graphs again once the steps in flight are done
+        VMAP_BCK(cudaDeviceSynchronize());
+        for (int i = 0; i < 2; ++i)
+            if (b->exec[i]) {
+                cudaGraphExecDestroy(b->exec[i]);
+                b->exec[i] = nullptr;
+            }
+        b->totalAllocTiles = b->totalNormalTiles = kFullGrid;
     }
-    *out = b;
+    b->maps[slot] = map;
     return VMAP_OK;
 }
 
@@ -152,6 +205,15 @@ vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void*
     for (int i = 0; i < n; ++i) {
         const vmap_batch_frame& f = frames[i];
         vmap_map* m = b->maps[i];
+        MapView& v = b->hViews[buf][i];
+        if (!m) {  // an empty slot takes no frame and contributes no work
+            if (f.depth_dev || f.vmap_dev || f.nmap_dev || f.rgb_dev) {
+                set_last_error("vmap_batch_step: frame " + std::to_string(i) + " given for an empty slot");
+                return VMAP_ERR_INVALID_ARG;
+            }
+            std::memset(&v, 0, sizeof(v));
+            continue;
+        }
         vmap_config c;
         vmap_get_config(m, &c);
         // a NULL depth frame skips this map's fusion, a NULL vertex map its
@@ -174,7 +236,6 @@ vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void*
             set_last_error("vmap_batch_step: invalid frame " + std::to_string(i));
             return VMAP_ERR_INVALID_ARG;
         }
-        MapView& v = b->hViews[buf][i];
         make_view(m, f.pose, v);
         v.in.active = fuse;
         v.in.depth = f.depth_dev;

@@ -19,6 +19,7 @@ struct vmap_map {
     DevMap dm;
     Launcher launcher;
     int device;
+    bool external;            // device buffers live in caller memory (vmap_create_in)
     size_t poolBytes;
     size_t deviceBytes;
     unsigned* hCtr;           // pinned readback of the counters
@@ -134,6 +135,26 @@ cudaError_t dalloc(vmap_map* m, T** p, size_t bytes)
     return e;
 }
 
+// Staging buffers of the host-buffer calls, allocated on the first such call
+// (maps driven only through device pointers never hold them).
+cudaError_t ensure_staging(vmap_map* m)
+{
+    if (m->dDepth) return cudaSuccess;
+    const size_t npix = (size_t)m->cfg.width * m->cfg.height, before = m->deviceBytes;
+    cudaError_t e = dalloc(m, &m->dDepth, npix * sizeof(float));
+    if (e == cudaSuccess) e = dalloc(m, &m->dRgb, npix * 3);
+    if (e == cudaSuccess) e = dalloc(m, &m->dVmap, npix * sizeof(float4));
+    if (e == cudaSuccess) e = dalloc(m, &m->dNmap, npix * sizeof(float4));
+    if (e != cudaSuccess) {
+        for (void* p : {m->dDepth, (void*)m->dRgb, (void*)m->dVmap, (void*)m->dNmap}) cudaFree(p);
+        m->deviceBytes = before;
+        m->dDepth = nullptr;
+        m->dRgb = nullptr;
+        m->dVmap = m->dNmap = nullptr;
+    }
+    return e;
+}
+
 void timing_free(vmap_map* m)
 {
     for (unsigned i = 0; i < 2 * m->tCap; ++i) cudaEventDestroy(m->tEv[i]);
@@ -161,20 +182,22 @@ cudaError_t staged(vmap_map* m, int stage, cudaStream_t s, F&& launch)
 void free_all(vmap_map* m)
 {
     timing_free(m);
-    cudaFree(m->dm.slots);
-    cudaFree(m->dm.blockKeys);
-    cudaFree(m->dm.pool);
-    cudaFree(m->dm.ctr);
-    cudaFree(m->dm.visList);
-    cudaFree(m->zmin);
-    cudaFree(m->zmax);
+    if (!m->external) {  // buffers carved from caller memory stay with the caller
+        cudaFree(m->dm.slots);
+        cudaFree(m->dm.blockKeys);
+        cudaFree(m->dm.pool);
+        cudaFree(m->dm.ctr);
+        cudaFree(m->dm.visList);
+        cudaFree(m->zmin);
+        cudaFree(m->zmax);
+        cudaFree(m->dNtri);
+    }
     cudaFree(m->dDepth);
     cudaFree(m->dRgb);
     cudaFree(m->dVmap);
     cudaFree(m->dNmap);
     cudaFree(m->dVerts);
     cudaFree(m->dNorms);
-    cudaFree(m->dNtri);
     if (m->hCtr) cudaFreeHost(m->hCtr);
     if (m->hVerts) cudaFreeHost(m->hVerts);
     if (m->hNorms) cudaFreeHost(m->hNorms);
@@ -269,18 +292,21 @@ size_t vmap_block_bytes(int fmt, int color)
     return 0;
 }
 
-vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
+}  // extern "C"
+
+namespace {
+
+// Validates a configuration and fills in its defaults (vmapping.cpp:57-75).
+vmap_status resolve_config(const vmap_config* cfg_in, vmap_config& cfg)
 {
-    if (!cfg_in || !out) return VMAP_ERR_INVALID_ARG;
-    *out = nullptr;
-    vmap_config cfg = *cfg_in;
+    if (!cfg_in) return VMAP_ERR_INVALID_ARG;
+    cfg = *cfg_in;
     if (cfg.width <= 0 || cfg.height <= 0 || !(cfg.fx > 0) || !(cfg.fy > 0) || !std::isfinite(cfg.cx) ||
         !std::isfinite(cfg.cy) || cfg.num_blocks <= 0 || !(cfg.voxel_size > 0) || cfg.num_entries < 0 ||
         cfg.num_buckets < 0 || cfg.truncation < 0 || cfg.max_weight < 0 || cfg.raycast_mode < 0 ||
         cfg.raycast_mode > 1)
         return VMAP_ERR_INVALID_ARG;
-    const size_t blockBytes = vmap_block_bytes(cfg.voxel_format, cfg.with_color);
-    if (blockBytes == 0) return VMAP_ERR_INVALID_ARG;
+    if (vmap_block_bytes(cfg.voxel_format, cfg.with_color) == 0) return VMAP_ERR_INVALID_ARG;
     if (cfg.num_buckets == 0) cfg.num_buckets = (int)(cfg.num_blocks * 0.9);  // vmapping.cpp:59
     if (cfg.num_buckets < 1) cfg.num_buckets = 1;
     if ((long long)cfg.num_buckets * kSlots < (long long)cfg.num_entries)
@@ -293,51 +319,76 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
     if (cfg.max_weight == 0) cfg.max_weight = 255;                 // depth_fusion.cu:193
     if (cfg.voxel_format == VMAP_VOXEL_REF && cfg.max_weight > 255) return VMAP_ERR_INVALID_ARG;
     if (cfg.max_weight > 65535) return VMAP_ERR_INVALID_ARG;
+    return VMAP_OK;
+}
 
+// Device buffers of a map, in order, each starting on a 256-byte boundary:
+// hash slots, block keys, voxel pool, counters, visible list, z-range tiles
+// (min, max), triangle count.
+struct MapLayout {
+    enum { SLOTS, KEYS, POOL, CTR, VIS, ZMIN, ZMAX, NTRI, N };
+    size_t off[N + 1];
+};
+
+MapLayout map_layout(const vmap_config& cfg)
+{
+    const size_t nslots = (size_t)cfg.num_buckets * kSlots, cap = (size_t)cfg.num_blocks;
+    const size_t ntiles = (size_t)((cfg.width + kZTile - 1) / kZTile) * ((cfg.height + kZTile - 1) / kZTile);
+    const size_t sz[MapLayout::N] = {nslots * sizeof(ulonglong2), cap * sizeof(unsigned long long),
+                                     cap * vmap_block_bytes(cfg.voxel_format, cfg.with_color),
+                                     C_COUNT * sizeof(unsigned), cap * sizeof(int),
+                                     ntiles * sizeof(unsigned long long), ntiles * sizeof(unsigned long long),
+                                     sizeof(unsigned)};
+    MapLayout l;
+    l.off[0] = 0;
+    for (int i = 0; i < MapLayout::N; ++i) l.off[i + 1] = (l.off[i] + sz[i] + 255) / 256 * 256;
+    return l;
+}
+
+// Builds a map for a resolved configuration. With `base` non-NULL its device
+// buffers are carved from the caller's memory (MapLayout) and the reset runs
+// asynchronously on `stream`; otherwise they are cudaMalloc'ed and the reset
+// is synchronous.
+vmap_status build_map(const vmap_config& cfg, unsigned char* base, cudaStream_t stream, vmap_map** out)
+{
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return (cuda_fail(e, "cudaGetDevice"), VMAP_ERR_NO_DEVICE);
-    cudaDeviceProp prop;
-    if ((e = cudaGetDeviceProperties(&prop, dev)) != cudaSuccess) return cuda_fail(e, "cudaGetDeviceProperties");
-    if (prop.major != 10) {
-        g_last_error = "libvmap_b200 is built for sm_100a; device is sm_" + std::to_string(prop.major * 10 + prop.minor);
+    int major = 0, sms = 0;
+    if ((e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev)) != cudaSuccess ||
+        (e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+        return cuda_fail(e, "cudaDeviceGetAttribute");
+    if (major != 10) {
+        g_last_error = "libvmap_b200 is built for sm_100a; device is sm_" + std::to_string(major * 10);
         return VMAP_ERR_NO_DEVICE;
     }
-
     vmap_map* m = new (std::nothrow) vmap_map();
     if (!m) return VMAP_ERR_OUT_OF_MEMORY;
     std::memset(m, 0, sizeof(*m));
     m->cfg = cfg;
     m->device = dev;
-    m->launcher.numSMs = prop.multiProcessorCount;
+    m->external = base != nullptr;
+    m->launcher.numSMs = sms;
     m->tilesX = (cfg.width + kZTile - 1) / kZTile;
     m->tilesY = (cfg.height + kZTile - 1) / kZTile;
-    const size_t nslots = (size_t)cfg.num_buckets * kSlots, cap = (size_t)cfg.num_blocks;
-    const size_t npix = (size_t)cfg.width * cfg.height, ntiles = (size_t)m->tilesX * m->tilesY;
-    m->poolBytes = cap * blockBytes;
-#define VMAP_ALLOC(ptr, bytes)                                        \
-    do {                                                              \
-        cudaError_t e2 = dalloc(m, &(ptr), (bytes));                  \
-        if (e2 != cudaSuccess) {                                      \
-            vmap_status st = cuda_fail(e2, "cudaMalloc " #ptr);        \
-            free_all(m);                                              \
-            delete m;                                                 \
-            return st;                                                \
-        }                                                             \
-    } while (0)
-    VMAP_ALLOC(m->dm.slots, nslots * sizeof(ulonglong2));
-    VMAP_ALLOC(m->dm.blockKeys, cap * sizeof(unsigned long long));
-    VMAP_ALLOC(m->dm.pool, m->poolBytes);
-    VMAP_ALLOC(m->dm.ctr, C_COUNT * sizeof(unsigned));
-    VMAP_ALLOC(m->dm.visList, cap * sizeof(int));
-    VMAP_ALLOC(m->zmin, ntiles * sizeof(unsigned long long));
-    VMAP_ALLOC(m->zmax, ntiles * sizeof(unsigned long long));
-    VMAP_ALLOC(m->dDepth, npix * sizeof(float));
-    VMAP_ALLOC(m->dRgb, npix * 3);
-    VMAP_ALLOC(m->dVmap, npix * sizeof(float4));
-    VMAP_ALLOC(m->dNmap, npix * sizeof(float4));
-    VMAP_ALLOC(m->dNtri, sizeof(unsigned));
-#undef VMAP_ALLOC
+    const size_t blockBytes = vmap_block_bytes(cfg.voxel_format, cfg.with_color);
+    m->poolBytes = (size_t)cfg.num_blocks * blockBytes;
+    const MapLayout l = map_layout(cfg);
+    void** ptrs[MapLayout::N] = {(void**)&m->dm.slots, (void**)&m->dm.blockKeys, (void**)&m->dm.pool,
+                                 (void**)&m->dm.ctr, (void**)&m->dm.visList, (void**)&m->zmin, (void**)&m->zmax,
+                                 (void**)&m->dNtri};
+    for (int i = 0; i < MapLayout::N; ++i) {
+        const size_t bytes = l.off[i + 1] - l.off[i];
+        if (base) {
+            *ptrs[i] = base + l.off[i];
+            m->deviceBytes += bytes;
+        } else if ((e = dalloc(m, (unsigned char**)ptrs[i], bytes)) != cudaSuccess) {
+            vmap_status st = cuda_fail(e, "cudaMalloc");
+            free_all(m);
+            delete m;
+            return st;
+        }
+    }
     if ((e = cudaHostAlloc((void**)&m->hCtr, C_COUNT * sizeof(unsigned), cudaHostAllocDefault)) != cudaSuccess) {
         vmap_status st = cuda_fail(e, "cudaHostAlloc");
         free_all(m);
@@ -352,8 +403,8 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
     m->dm.mu = cfg.truncation;
     m->dm.wmax = (float)cfg.max_weight;
     m->epoch = 0xFFFFFFFEu;  // the first render re-initialises the tiles
-    vmap_status st = vmap_reset(m, nullptr);
-    if (st == VMAP_OK && (e = cudaStreamSynchronize(nullptr)) != cudaSuccess) st = cuda_fail(e, "create sync");
+    vmap_status st = vmap_reset(m, stream);
+    if (st == VMAP_OK && !base && (e = cudaStreamSynchronize(stream)) != cudaSuccess) st = cuda_fail(e, "create sync");
     if (st != VMAP_OK) {
         free_all(m);
         delete m;
@@ -363,10 +414,50 @@ vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
     return VMAP_OK;
 }
 
+}  // namespace
+
+extern "C" {
+
+vmap_status vmap_create(const vmap_config* cfg_in, vmap_map** out)
+{
+    if (!cfg_in || !out) return VMAP_ERR_INVALID_ARG;
+    *out = nullptr;
+    vmap_config cfg;
+    vmap_status st = resolve_config(cfg_in, cfg);
+    if (st != VMAP_OK) return st;
+    return build_map(cfg, nullptr, nullptr, out);
+}
+
+vmap_status vmap_required_bytes(const vmap_config* cfg_in, uint64_t* bytes)
+{
+    if (!cfg_in || !bytes) return VMAP_ERR_INVALID_ARG;
+    vmap_config cfg;
+    vmap_status st = resolve_config(cfg_in, cfg);
+    if (st != VMAP_OK) return st;
+    *bytes = map_layout(cfg).off[MapLayout::N];
+    return VMAP_OK;
+}
+
+vmap_status vmap_create_in(const vmap_config* cfg_in, void* device_mem, uint64_t bytes, void* stream,
+                           vmap_map** out)
+{
+    if (!cfg_in || !out || !device_mem || ((uintptr_t)device_mem & 255)) return VMAP_ERR_INVALID_ARG;
+    *out = nullptr;
+    vmap_config cfg;
+    vmap_status st = resolve_config(cfg_in, cfg);
+    if (st != VMAP_OK) return st;
+    if (bytes < map_layout(cfg).off[MapLayout::N]) {
+        g_last_error = "vmap_create_in: " + std::to_string(bytes) + " bytes given, " +
+                       std::to_string(map_layout(cfg).off[MapLayout::N]) + " needed";
+        return VMAP_ERR_INVALID_ARG;
+    }
+    return build_map(cfg, static_cast<unsigned char*>(device_mem), as_stream(stream), out);
+}
+
 vmap_status vmap_destroy(vmap_map* m)
 {
     if (!m) return VMAP_ERR_INVALID_ARG;
-    cudaDeviceSynchronize();
+    if (!m->external) cudaDeviceSynchronize();
     free_all(m);
     delete m;
     return VMAP_OK;
@@ -441,6 +532,7 @@ vmap_status vmap_fuse_host(vmap_map* m, const void* depth_host, int depth_type, 
     cudaStream_t s = as_stream(stream);
     const size_t npix = (size_t)m->cfg.width * m->cfg.height;
     const size_t elem = depth_type == VMAP_DEPTH_F32 ? 4 : 2;
+    VMAP_CK(ensure_staging(m));
     VMAP_CK(cudaMemcpyAsync(m->dDepth, depth_host, npix * elem, cudaMemcpyHostToDevice, s));
     if (rgb_host) VMAP_CK(cudaMemcpyAsync(m->dRgb, rgb_host, npix * 3, cudaMemcpyHostToDevice, s));
     return fuse_impl(m, m->dDepth, depth_type, elem * m->cfg.width, depth_scale, rgb_host ? m->dRgb : nullptr,
@@ -494,6 +586,7 @@ vmap_status vmap_render_scene_host(vmap_map* m, const double pose[16], float* vm
 {
     if (!m || !vmap_host) return VMAP_ERR_INVALID_ARG;
     cudaStream_t s = as_stream(stream);
+    VMAP_CK(ensure_staging(m));
     vmap_status st = vmap_render_scene(m, pose, (float*)m->dVmap, 0, nmap_host ? (float*)m->dNmap : nullptr, 0, stream);
     if (st != VMAP_OK) return st;
     const size_t bytes = (size_t)m->cfg.width * m->cfg.height * sizeof(float4);

@@ -165,10 +165,11 @@ __global__ void __launch_bounds__(256) mesh_kernel(DevMap m, float* verts, float
     }
 }
 
-__global__ void mesh_finish_kernel(DevMap m, unsigned maxTris, unsigned* ntrisOut)
+// A pass without an output buffer only counts: it flags nothing.
+__global__ void mesh_finish_kernel(DevMap m, unsigned maxTris, unsigned* ntrisOut, bool emitting)
 {
     const unsigned n = m.ctr[C_TRI];
-    if (n > maxTris) atomicOr(m.ctr + C_ERR, VMAP_FLAG_BUFFER_FULL);
+    if (emitting && n > maxTris) atomicOr(m.ctr + C_ERR, VMAP_FLAG_BUFFER_FULL);
     if (ntrisOut) *ntrisOut = n;
 }
 
@@ -227,7 +228,7 @@ cudaError_t launch_mesh(const DevMap& m, int fmt, float* verts, float* norms, un
     default: return cudaErrorInvalidValue;
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    mesh_finish_kernel<<<1, 1, 0, s>>>(m, maxTris, ntrisOut);
+    mesh_finish_kernel<<<1, 1, 0, s>>>(m, maxTris, ntrisOut, verts != nullptr);
     return cudaGetLastError();
 }
 

@@ -1,0 +1,478 @@
+"""Serving many mapping sessions from one GPU.
+
+A session is one map (its own scene, camera, voxel size and pool). Requests
+arrive over time: "fuse" (a depth + colour frame to integrate), "raycast"
+(render the vertex + normal maps at a pose and return them to the host) and
+"mesh" (extract the full triangle mesh to the host). The reference serves a
+single map per process and has no counterpart; this module adds the server
+around the library's batch step (vmap_batch_step) and map snapshots
+(vmap_snapshot_save / vmap_snapshot_load).
+
+Scheduling works in ticks. A tick takes, for every session with waiting
+requests, the oldest one (a fuse directly followed by a raycast of the same
+session goes into the same tick: one batch frame fuses, then renders), runs
+all of them as ONE batch step over the resident maps (maps without work are
+idle in that step), copies raycast results to pinned host memory, then runs
+at most `max_mesh_per_tick` mesh requests. Requests of one session complete
+in arrival order.
+
+Admission is by device memory: a session's map (voxel-block pool, hash table,
+frame buffers) must be resident to serve it. A non-resident session is
+admitted if its bytes fit the budget, evicting least-recently-used idle
+sessions (snapshot to pinned host memory, map released) as needed; if they
+still do not fit, its requests wait. At most VMAP_MAX_BATCH (256) maps are
+resident, the batch step's limit.
+
+`Scheduler` is pure host logic (tested on the CPU with a fake executor);
+`GpuExecutor` drives the library.
+"""
+import collections
+import ctypes as C
+import dataclasses
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+
+KINDS = ("fuse", "raycast", "mesh")
+MAX_RESIDENT = 256
+
+
+@dataclass
+class Request:
+    kind: str
+    session: int
+    arrival: float            # seconds after the start of the run
+    index: int = 0            # position in the arrival order
+    done: float = math.nan    # completion time, seconds after the start
+    tick: int = -1
+    result: object = None
+
+    @property
+    def latency(self):
+        return self.done - self.arrival
+
+
+def poisson_requests(n_sessions, rate, count, mix=(0.70, 0.25, 0.05), seed=0):
+    """`count` requests with exponential inter-arrival times at `rate` per
+    second, sessions uniform at random, kinds drawn with probabilities `mix`
+    (fuse, raycast, mesh)."""
+    rng = np.random.default_rng(seed)
+    t = np.cumsum(rng.exponential(1.0 / rate, count))
+    sess = rng.integers(0, n_sessions, count)
+    kinds = rng.choice(len(KINDS), count, p=np.asarray(mix, np.float64) / np.sum(mix))
+    return [Request(KINDS[k], int(s), float(a), i) for i, (k, s, a) in enumerate(zip(kinds, sess, t))]
+
+
+@dataclass
+class TickPlan:
+    batch: list = field(default_factory=list)    # (session, fuse request or None, raycast request or None)
+    mesh: list = field(default_factory=list)     # mesh requests
+    evict: list = field(default_factory=list)    # sessions to evict before the tick
+    restore: list = field(default_factory=list)  # sessions to make resident before the tick
+
+    def requests(self):
+        out = [r for _, f, q in self.batch for r in (f, q) if r is not None]
+        return out + list(self.mesh)
+
+
+class Scheduler:
+    """Admission, eviction and tick formation (no GPU work).
+
+    session_bytes[s] is the device memory session s holds while resident;
+    budget the bytes all resident sessions may hold together."""
+
+    def __init__(self, session_bytes, budget, max_mesh_per_tick=2, max_resident=MAX_RESIDENT):
+        self.bytes = list(session_bytes)
+        if max(self.bytes) > budget:
+            raise ValueError("a session needs more device memory than the whole budget")
+        self.budget = budget
+        self.max_mesh = max_mesh_per_tick
+        self.max_resident = max_resident
+        self.resident = collections.OrderedDict()  # session -> None, least recently used first
+        self.used = 0
+        self.queues = collections.defaultdict(collections.deque)  # session -> waiting requests
+        self.waiting = 0
+        self.evictions = 0
+        self.restores = 0
+
+    def submit(self, req):
+        self.queues[req.session].append(req)
+        self.waiting += 1
+
+    def free(self):
+        return self.budget - self.used
+
+    def plan(self):
+        """Take the next tick's work off the queues."""
+        p = TickPlan()
+        heads = sorted((q[0].arrival, s) for s, q in self.queues.items() if q)
+        busy = set()
+        for _, s in heads:
+            q = self.queues[s]
+            if q[0].kind == "mesh" and len(p.mesh) >= self.max_mesh:
+                continue
+            if s not in self.resident and (s in p.evict or not self._admit(s, busy, p)):
+                continue
+            busy.add(s)
+            self.resident.move_to_end(s)
+            head = q.popleft()
+            self.waiting -= 1
+            if head.kind == "mesh":
+                p.mesh.append(head)
+            elif head.kind == "raycast":
+                p.batch.append((s, None, head))
+            else:
+                ray = None
+                if q and q[0].kind == "raycast":
+                    ray = q.popleft()
+                    self.waiting -= 1
+                p.batch.append((s, head, ray))
+        return p
+
+    def _admit(self, s, busy, p):
+        need = self.bytes[s]
+        # idle sessions, least recently used first; those without waiting work before the rest
+        idle = [v for v in self.resident if v not in busy]
+        victims = [v for v in idle if not self.queues[v]] + [v for v in idle if self.queues[v]]
+        freed, take = 0, []
+        for v in victims:
+            if self.free() + freed >= need and len(self.resident) - len(take) < self.max_resident:
+                break
+            take.append(v)
+            freed += self.bytes[v]
+        if self.free() + freed < need or len(self.resident) - len(take) >= self.max_resident:
+            return False
+        for v in take:
+            del self.resident[v]
+            self.used -= self.bytes[v]
+            p.evict.append(v)
+            self.evictions += 1
+        self.resident[s] = None
+        self.used += need
+        p.restore.append(s)
+        self.restores += 1
+        return True
+
+
+class GpuExecutor:
+    """Runs tick plans on the GPU.
+
+    All resident maps sit in the slots of ONE long-lived slot batch
+    (vmap_batch_create_slots), so its recorded CUDA graphs are reused whatever
+    sessions come and go. A resident session owns a device block from torch's
+    caching allocator holding its map (vmap_create_in: creating and
+    destroying maps allocates and frees no device memory) plus buffers for one
+    frame and one vertex + normal map; an evicted session owns a snapshot in
+    pinned host memory. Frames are pre-rendered into pinned host memory
+    (frames[s] = list of (depth int16 (h, w), rgb uint8 (h, 3w), pose (4, 4)))
+    and copied in per fuse request. Meshes are extracted on the device into
+    shared buffers and copied to one pinned host buffer."""
+
+    def __init__(self, workloads, frames, device="cuda", copy_results=True, keep_results=False,
+                 n_slots=MAX_RESIDENT):
+        import torch
+        self.torch = torch
+        self.wls = list(workloads)
+        self.frames = frames
+        self.dev = torch.device(device)
+        self.stream = torch.cuda.Stream(device=self.dev)
+        self.sp = C.c_void_p(self.stream.cuda_stream)
+        self.copy_results = copy_results
+        self.keep_results = keep_results  # fresh host buffers per raycast (tests), else one pair per session
+        self.lib = L.lib()
+        fmts = {w.voxel_format for w in self.wls}
+        if len(fmts) != 1:
+            raise ValueError("all sessions need one voxel format")
+        self.n_slots = min(n_slots, MAX_RESIDENT)
+        h = C.c_void_p()
+        L.check(self.lib.vmap_batch_create_slots(self.n_slots, L.FORMAT_NAMES[fmts.pop()], C.byref(h)),
+                "vmap_batch_create_slots")
+        self.batch = h
+        self.frames_arr = (L.BatchFrame * self.n_slots)()
+        self.free_slots = list(range(self.n_slots - 1, -1, -1))
+        self.slot = {}       # session -> batch slot (resident)
+        self.maps = {}       # session -> VoxelMapping (resident)
+        self.bufs = {}       # session -> (depth, rgb, vmap, nmap) device tensors
+        self.snaps = {}      # session -> pinned uint8 snapshot
+        self.outs = {}       # session -> (vmap, nmap) pinned host results
+        self.next_frame = collections.Counter()
+        self.dirty = []      # slots whose frame pointers the last tick set
+        self.mesh_dev = None  # (verts, norms) device buffers, grown on demand
+        self.mesh_host = None
+        self.mesh_count = torch.zeros(1, dtype=torch.int32, device=self.dev)
+        self.mesh_count_host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
+        self.phase = collections.Counter()  # seconds per phase
+
+    # -- memory ----------------------------------------------------------------
+    def _new_map(self, s):
+        from .vmapping import VoxelMapping
+        w = self.wls[s]
+        return VoxelMapping(w.width, w.height, w.K, voxel_format=w.voxel_format, with_color=w.with_color,
+                            max_weight=w.max_weight)
+
+    def map_bytes(self, s):
+        w = self.wls[s]
+        return self._new_map(s).required_bytes(w.num_entries, w.num_blocks, w.voxel_size)
+
+    def session_bytes(self, s):
+        """Device bytes of session s while resident: its map
+        (vmap_required_bytes) plus its frame and vertex / normal map buffers."""
+        w = self.wls[s]
+        return self.map_bytes(s) + w.width * w.height * (2 + 3 + 16 + 16)
+
+    def restore(self, s):
+        torch = self.torch
+        w = self.wls[s]
+        with torch.cuda.stream(self.stream):
+            mem = torch.empty(self.map_bytes(s), dtype=torch.uint8, device=self.dev)
+            vm = self._new_map(s)
+            vm.CreateMapIn(w.num_entries, w.num_blocks, w.voxel_size, mem)
+            if s in self.snaps:
+                vm.load_snapshot(self.snaps[s])
+            self.bufs[s] = (torch.empty((w.height, w.width), dtype=torch.int16, device=self.dev),
+                            torch.empty((w.height, w.width * 3), dtype=torch.uint8, device=self.dev),
+                            torch.empty((w.height, w.width, 4), dtype=torch.float32, device=self.dev),
+                            torch.empty((w.height, w.width, 4), dtype=torch.float32, device=self.dev))
+        slot = self.free_slots.pop()
+        L.check(self.lib.vmap_batch_set_map(self.batch, slot, vm._map), "vmap_batch_set_map")
+        self.maps[s], self.slot[s] = vm, slot
+        f = self.frames_arr[slot]
+        f.depth_type, f.depth_pitch, f.depth_scale = L.DEPTH_U16, w.width * 2, w.depth_scale
+        f.rgb_pitch, f.vmap_pitch, f.nmap_pitch = w.width * 3, w.width * 16, w.width * 16
+
+    def evict(self, s):
+        torch = self.torch
+        vm = self.maps.pop(s)
+        slot = self.slot.pop(s)
+        with torch.cuda.stream(self.stream):
+            n = vm.snapshot_bytes()
+            buf = self.snaps.get(s)
+            if buf is None or buf.numel() < n:
+                buf = torch.empty(max(n, 1 << 16) * 5 // 4, dtype=torch.uint8, pin_memory=True)
+            self.snaps[s] = buf[:vm.save_snapshot(buf).shape[0]]  # synchronous
+        L.check(self.lib.vmap_batch_set_map(self.batch, slot, None), "vmap_batch_set_map")
+        vm.release()  # the map's memory returns to torch's cache; nothing of it is in flight
+        self.bufs.pop(s)
+        self.free_slots.append(slot)
+        f = self.frames_arr[slot]
+        f.depth_dev = f.rgb_dev = f.vmap_dev = f.nmap_dev = None
+
+    # -- one tick ----------------------------------------------------------------
+    def _mesh(self, s):
+        """Full mesh of session s to pinned host memory; returns the triangle count."""
+        torch = self.torch
+        vm = self.maps[s]
+        lib = self.lib
+        L.check(lib.vmap_polygonize(vm._map, None, None, 0, C.c_void_p(self.mesh_count.data_ptr()), self.sp),
+                "vmap_polygonize")
+        self.mesh_count_host.copy_(self.mesh_count, non_blocking=True)
+        self.stream.synchronize()
+        n = int(self.mesh_count_host.item())
+        if n == 0:
+            return 0
+        if self.mesh_dev is None or self.mesh_dev[0].shape[0] < n:
+            cap = max(n * 5 // 4, 1 << 16)
+            self.mesh_dev = (torch.empty((cap, 9), dtype=torch.float32, device=self.dev),
+                             torch.empty((cap, 9), dtype=torch.float32, device=self.dev))
+            self.mesh_host = (torch.empty((cap, 9), dtype=torch.float32, pin_memory=True),
+                              torch.empty((cap, 9), dtype=torch.float32, pin_memory=True))
+        v, nr = self.mesh_dev
+        L.check(lib.vmap_polygonize(vm._map, C.c_void_p(v.data_ptr()), C.c_void_p(nr.data_ptr()), v.shape[0],
+                                    None, self.sp), "vmap_polygonize")
+        self.mesh_host[0][:n].copy_(v[:n], non_blocking=True)
+        self.mesh_host[1][:n].copy_(nr[:n], non_blocking=True)
+        self.stream.synchronize()
+        return n
+
+    def run_tick(self, plan, clock):
+        """Executes `plan`; sets each request's completion time from `clock()`."""
+        torch = self.torch
+        t0 = clock()
+        for s in plan.evict:
+            self.evict(s)
+        t1 = clock()
+        for s in plan.restore:
+            self.restore(s)
+        t2 = clock()
+        self.phase["evict"] += t1 - t0
+        self.phase["restore"] += t2 - t1
+        with torch.cuda.stream(self.stream):
+            if plan.batch:
+                for i in self.dirty:
+                    f = self.frames_arr[i]
+                    f.depth_dev = f.rgb_dev = f.vmap_dev = f.nmap_dev = None
+                self.dirty = []
+                for s, fuse, ray in plan.batch:
+                    slot = self.slot[s]
+                    f = self.frames_arr[slot]
+                    self.dirty.append(slot)
+                    d_dev, c_dev, v_dev, n_dev = self.bufs[s]
+                    if fuse is not None:
+                        k = self.next_frame[s] % len(self.frames[s])
+                        self.next_frame[s] += 1
+                        d, c, pose = self.frames[s][k]
+                        d_dev.copy_(d, non_blocking=True)
+                        c_dev.copy_(c, non_blocking=True)
+                        f.depth_dev, f.rgb_dev = d_dev.data_ptr(), c_dev.data_ptr()
+                    else:
+                        k = max(self.next_frame[s] - 1, 0) % len(self.frames[s])
+                        pose = self.frames[s][k][2]
+                    f.pose[:] = [float(x) for x in np.asarray(pose, np.float64).reshape(16)]
+                    if ray is not None:
+                        f.vmap_dev, f.nmap_dev = v_dev.data_ptr(), n_dev.data_ptr()
+                L.check(self.lib.vmap_batch_step(self.batch, self.frames_arr, self.sp), "vmap_batch_step")
+                for s, fuse, ray in plan.batch:
+                    if ray is not None and self.copy_results:
+                        out = None if self.keep_results else self.outs.get(s)
+                        _, _, v_dev, n_dev = self.bufs[s]
+                        if out is None:
+                            out = (torch.empty(v_dev.shape, dtype=torch.float32, pin_memory=True),
+                                   torch.empty(n_dev.shape, dtype=torch.float32, pin_memory=True))
+                            if not self.keep_results:
+                                self.outs[s] = out
+                        out[0].copy_(v_dev, non_blocking=True)
+                        out[1].copy_(n_dev, non_blocking=True)
+                        ray.result = (out[0], out[1], self.next_frame[s])  # maps + frames fused so far
+                self.stream.synchronize()
+                t = clock()
+                for r in plan.requests():
+                    if r.kind != "mesh":
+                        r.done = t
+            t3 = clock()
+            self.phase["batch"] += t3 - t2
+            for r in plan.mesh:
+                r.result = self._mesh(r.session)
+                r.done = clock()
+            self.phase["mesh"] += clock() - t3
+
+    def release(self):
+        self.torch.cuda.synchronize()
+        for s in list(self.maps):
+            L.check(self.lib.vmap_batch_set_map(self.batch, self.slot[s], None), "vmap_batch_set_map")
+            self.maps.pop(s).release()
+        self.slot.clear()
+        if self.batch is not None:
+            L.check(self.lib.vmap_batch_destroy(self.batch), "vmap_batch_destroy")
+            self.batch = None
+
+
+def serve(requests, scheduler, executor, clock=None, wait_until=None):
+    """Replays `requests` (sorted by arrival) against wall-clock time: a
+    request becomes visible to the scheduler at its arrival time; ticks run
+    back to back while work is waiting. `clock` / `wait_until` replace the
+    wall clock and the idle wait (for simulated time). Returns
+    (requests, stats)."""
+    start = time.perf_counter()
+    clock = clock or (lambda: time.perf_counter() - start)
+
+    def sleep_until(t):
+        while True:
+            wait = t - clock()
+            if wait <= 0:
+                return
+            if wait > 2e-4:
+                time.sleep(wait - 1e-4)
+
+    wait_until = wait_until or sleep_until
+    pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
+    ticks, batch_sizes, busy = 0, [], 0.0
+    while pending or scheduler.waiting:
+        now = clock()
+        while pending and pending[0].arrival <= now:
+            scheduler.submit(pending.popleft())
+        if not scheduler.waiting:
+            wait_until(pending[0].arrival)
+            continue
+        plan = scheduler.plan()
+        if not plan.batch and not plan.mesh:
+            raise RuntimeError("no admissible work: the budget cannot hold any waiting session")
+        t0 = clock()
+        executor.run_tick(plan, clock)
+        busy += clock() - t0
+        for r in plan.requests():
+            r.tick = ticks
+        ticks += 1
+        batch_sizes.append(len(plan.batch))
+    makespan = clock()
+    stats = {"ticks": ticks, "mean_batch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
+             "max_batch": int(max(batch_sizes)) if batch_sizes else 0, "busy_s": busy, "makespan_s": makespan,
+             "evictions": scheduler.evictions, "restores": scheduler.restores}
+    return requests, stats
+
+
+def summarize(requests, stats):
+    """Throughput and latency percentiles (ms) per request kind."""
+    out = {"requests": len(requests), "throughput_rps": len(requests) / stats["makespan_s"]}
+    for kind in KINDS + ("all",):
+        lat = [r.latency for r in requests if kind in ("all", r.kind)]
+        if lat:
+            out[kind] = {"n": len(lat), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+                         "p99_ms": 1e3 * float(np.percentile(lat, 99)), "mean_ms": 1e3 * float(np.mean(lat))}
+    out.update(stats)
+    return out
+
+
+def render_frames(workloads, n_frames, pin=True):
+    """n_frames frames per workload, spread over its trajectory, as pinned
+    host tensors: [(depth int16 (h, w), rgb uint8 (h, 3w), pose (4, 4)), ...]."""
+    import torch
+    from . import synth
+    out = []
+    for w in workloads:
+        sc = synth.Scene(w)
+        stride = max(1, w.n_poses // n_frames)
+        fr = []
+        for i in range(n_frames):
+            d, c, p = sc.render(i * stride)
+            dt = torch.from_numpy(d.view(np.int16))
+            ct = torch.from_numpy(c).reshape(w.height, -1)
+            fr.append((dt.pin_memory() if pin else dt, ct.pin_memory() if pin else ct, p))
+        out.append(fr)
+    return out
+
+
+def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, budget_frac=0.5, n_frames=4,
+                seed=0, warmup=500, max_mesh_per_tick=2, keep_results=False, pool_scale=1, log=None):
+    """Builds n_sessions uneven sessions (FP16 + colour), then for each rate
+    replays `count` Poisson requests (70/25/5 fuse/raycast/mesh) after a
+    warm-up of `warmup` requests. The budget is `budget_bytes`, or
+    `budget_frac` of all sessions' bytes, capped at 85 % of the free device
+    memory. `pool_scale` multiplies every pool. Returns (list of per-rate
+    summaries, executor)."""
+    import torch
+    from . import synth
+    wls = [dataclasses.replace(w, num_blocks=w.num_blocks * pool_scale)
+           for w in synth.uneven_workloads(n_sessions, seed=seed)]
+    frames = render_frames(wls, n_frames)
+    ex = GpuExecutor(wls, frames, keep_results=keep_results)
+    sizes = [ex.session_bytes(s) for s in range(n_sessions)]
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(budget_bytes or budget_frac * sum(sizes))
+    budget = max(max(sizes), min(budget, int(0.85 * free)))
+    results = []
+    try:
+        sched = Scheduler(sizes, budget, max_mesh_per_tick=max_mesh_per_tick)
+        if warmup:
+            serve(poisson_requests(n_sessions, max(rates), warmup, seed=seed + 7), sched, ex)
+        for k, rate in enumerate(rates):
+            sched.evictions = sched.restores = 0
+            reqs = poisson_requests(n_sessions, rate, count, seed=seed + 100 + k)
+            ex.phase.clear()
+            reqs, stats = serve(reqs, sched, ex)
+            summ = summarize(reqs, stats)
+            summ["phase_s"] = {k: round(v, 4) for k, v in ex.phase.items()}
+            summ.update({"offered_rps": rate, "sessions": n_sessions, "budget_gb": budget / 1e9,
+                         "all_sessions_gb": sum(sizes) / 1e9})
+            results.append(summ)
+            if log:
+                log(summ)
+            if keep_results:
+                summ["_requests"] = reqs
+    except BaseException:
+        ex.release()
+        raise
+    return results, ex

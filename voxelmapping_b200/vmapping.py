@@ -44,24 +44,51 @@ class VoxelMapping:
         self.raycast_mode = int(raycast_mode)
         self.num_buckets = int(num_buckets)
         self._map = None
+        self._mem = None
         self._lib = L.lib()
 
     # -- lifetime ------------------------------------------------------------
+    def _config(self, numEntries, numVoxels, voxelSize):
+        return L.Config(self.width, self.height, float(self.K[0, 0]), float(self.K[1, 1]), float(self.K[0, 2]),
+                        float(self.K[1, 2]), int(numEntries), int(numVoxels), float(voxelSize), self.num_buckets,
+                        self.truncation, self.voxel_format, self.max_weight, int(self.with_color), self.raycast_mode)
+
     def CreateMap(self, numEntries, numVoxels, voxelSize):
         """vmapping.cpp:57-75: allocate and reset the map."""
         self.release()
-        cfg = L.Config(self.width, self.height, float(self.K[0, 0]), float(self.K[1, 1]), float(self.K[0, 2]),
-                       float(self.K[1, 2]), int(numEntries), int(numVoxels), float(voxelSize), self.num_buckets,
-                       self.truncation, self.voxel_format, self.max_weight, int(self.with_color), self.raycast_mode)
+        cfg = self._config(numEntries, numVoxels, voxelSize)
         h = C.c_void_p()
         L.check(self._lib.vmap_create(C.byref(cfg), C.byref(h)), "vmap_create")
         self._map = h
+        self.config = self.get_config()
+
+    def required_bytes(self, numEntries, numVoxels, voxelSize):
+        """Device bytes CreateMapIn needs for this map (vmap_required_bytes)."""
+        n = C.c_uint64()
+        L.check(self._lib.vmap_required_bytes(C.byref(self._config(numEntries, numVoxels, voxelSize)), C.byref(n)),
+                "vmap_required_bytes")
+        return n.value
+
+    def CreateMapIn(self, numEntries, numVoxels, voxelSize, memory):
+        """CreateMap inside `memory`, a CUDA uint8 tensor of at least
+        required_bytes() (vmap_create_in; the reset is asynchronous on the
+        current stream). The map keeps a reference to the tensor until
+        release(), which the caller calls only once the map's work is done."""
+        self.release()
+        cfg = self._config(numEntries, numVoxels, voxelSize)
+        h = C.c_void_p()
+        L.check(self._lib.vmap_create_in(C.byref(cfg), C.c_void_p(memory.data_ptr()),
+                                         memory.numel() * memory.element_size(), _stream(), C.byref(h)),
+                "vmap_create_in")
+        self._map = h
+        self._mem = memory
         self.config = self.get_config()
 
     def release(self):
         if self._map is not None:
             L.check(self._lib.vmap_destroy(self._map), "vmap_destroy")
             self._map = None
+        self._mem = None
 
     def __del__(self):
         try:
