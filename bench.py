@@ -182,11 +182,18 @@ def run_reference(args):
 
 
 # -------------------------------------------------------------- batched arm
-def run_batched(args, wls, dev, flush, world, plain_value, distinct_frames=None):
+def run_batched(args, wls, dev, flush, world, distinct_frames=None):
     """One map per workload in `wls` (one voxel format for all), each fed its
     own seeded scene; one vmap_batch_step per step (one launch per stage over
     all maps, graph-replayed on a side stream). With `distinct_frames` F, each
-    map renders F frames and the steps cycle through them."""
+    map renders F frames and the steps cycle through them.
+
+    The same maps' frames are then run through the plain path: FP32 TSDF +
+    float weight + colour maps, one map per call (vmap_fuse_depth_rgb +
+    vmap_render_scene, six launches per map), same steps, same L2 flush;
+    `ratio_vs_plain` compares the two on identical work."""
+    import dataclasses
+
     import torch
     import torch.distributed as dist
     from voxelmapping_b200 import MapBatch, VoxelMapping
@@ -198,7 +205,7 @@ def run_batched(args, wls, dev, flush, world, plain_value, distinct_frames=None)
     W = min(args.warmup, 5)
     nfr = W + K
     F = min(nfr, distinct_frames or nfr)
-    maps, depth, rgb, poses, vmaps, nmaps = [], [], [], [], [], []
+    depth, rgb, poses, vmaps, nmaps = [], [], [], [], []
     for b, w in enumerate(wls):
         sc = synth.Scene(w)
         d_b = torch.empty((F, w.height, w.width), dtype=torch.int16, device=dev)
@@ -215,10 +222,44 @@ def run_batched(args, wls, dev, flush, world, plain_value, distinct_frames=None)
         depth.append(d_b), rgb.append(c_b), poses.append(p_b)
         vmaps.append(torch.empty((w.height, w.width, 4), dtype=torch.float32, device=dev))
         nmaps.append(torch.empty((w.height, w.width, 4), dtype=torch.float32, device=dev))
-        vm = VoxelMapping(w.width, w.height, w.K, voxel_format=w.voxel_format, with_color=w.with_color,
-                          max_weight=w.max_weight)
-        vm.CreateMap(w.num_entries, w.num_blocks, w.voxel_size)
-        maps.append(vm)
+
+    def make_maps(fmt_wls):
+        maps = []
+        for w in fmt_wls:
+            vm = VoxelMapping(w.width, w.height, w.K, voxel_format=w.voxel_format, with_color=w.with_color,
+                              max_weight=w.max_weight)
+            vm.CreateMap(w.num_entries, w.num_blocks, w.voxel_size)
+            maps.append(vm)
+        return maps
+
+    lib = L.lib()
+    side = torch.cuda.Stream(device=dev)
+    sp = C.c_void_p(side.cuda_stream)
+
+    def timed(run_step):
+        """W untimed + K timed steps on the side stream; per-step ms (max over ranks of the sum)."""
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            for i in range(W):
+                run_step(i)
+            side.synchronize()
+            if world > 1:
+                dist.barrier()
+            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+            for k in range(K):
+                flush.fill_(k & 255)
+                ev[k][0].record(side)
+                run_step(W + k)
+                ev[k][1].record(side)
+            side.synchronize()
+        step_ms = [a.elapsed_time(b) for a, b in ev]
+        t = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return step_ms, float(t.item())
+
+    # --- batched: one vmap_batch_step over all maps per step
+    maps = make_maps(wls)
     batch = MapBatch(maps)
     frames = []
     for i in range(nfr):
@@ -234,38 +275,41 @@ def run_batched(args, wls, dev, flush, world, plain_value, distinct_frames=None)
             f.vmap_dev, f.vmap_pitch = vmaps[b].data_ptr(), w.width * 16
             f.nmap_dev, f.nmap_pitch = nmaps[b].data_ptr(), w.width * 16
         frames.append(fr)
-    lib = L.lib()
-    side = torch.cuda.Stream(device=dev)
-    sp = C.c_void_p(side.cuda_stream)
-    torch.cuda.synchronize()
-    with torch.cuda.stream(side):
-        for i in range(W):
-            L.check(lib.vmap_batch_step(batch._h, frames[i], sp))
-        side.synchronize()
-        if world > 1:
-            dist.barrier()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
-        for k in range(K):
-            flush.fill_(k & 255)
-            ev[k][0].record(side)
-            L.check(lib.vmap_batch_step(batch._h, frames[W + k], sp))
-            ev[k][1].record(side)
-        side.synchronize()
-    step_ms = [a.elapsed_time(b) for a, b in ev]
-    t = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    value = world * B * K / (float(t.item()) / 1e3)
+    step_ms, tot = timed(lambda i: L.check(lib.vmap_batch_step(batch._h, frames[i], sp)))
+    value = world * B * K / (tot / 1e3)
     pixels = sum(w.width * w.height for w in wls)
     hits = float(sum(torch.isfinite(v[..., 0]).sum().item() for v in vmaps)) / pixels
     stats = [m.stats() for m in maps]
     batch.release()
     for m in maps:
         m.release()
+
+    # --- plain: the same frames, FP32 maps, one map per call
+    pwls = [dataclasses.replace(w, voxel_format="f32", max_weight=255) for w in wls]
+    pmaps = make_maps(pwls)
+    pargs = [[L.pose_arg(poses[b][j].reshape(4, 4)) for j in range(F)] for b in range(B)]
+
+    def plain_step(i):
+        j = i % F
+        for b, (w, vm) in enumerate(zip(pwls, pmaps)):
+            L.check(lib.vmap_fuse_depth_rgb(vm._map, depth[b][j].data_ptr(), L.DEPTH_U16, w.width * 2, w.depth_scale,
+                                            rgb[b][j].data_ptr() if rgb[b] is not None else None, w.width * 3,
+                                            pargs[b][j], sp))
+            L.check(lib.vmap_render_scene(vm._map, pargs[b][j], vmaps[b].data_ptr(), w.width * 16,
+                                          nmaps[b].data_ptr(), w.width * 16, sp))
+
+    p_ms, p_tot = timed(plain_step)
+    p_value = world * B * K / (p_tot / 1e3)
+    for m in pmaps:
+        m.release()
     return {"value": value, "unit": "frames/s", "maps": B, "steps": K, "warmup": W,
-            "ms_per_step": float(t.item()) / K, "p50_ms_per_step": percentile(step_ms, 50),
-            "p99_ms_per_step": percentile(step_ms, 99), "ratio_vs_plain": value / plain_value,
-            "megapixels_per_step": pixels / 1e6, "dtype": wls[0].voxel_format,
+            "ms_per_step": tot / K, "p50_ms_per_step": percentile(step_ms, 50),
+            "p99_ms_per_step": percentile(step_ms, 99),
+            "plain_same_frames": {"value": p_value, "unit": "frames/s", "ms_per_step": p_tot / K,
+                                  "p50_ms_per_step": percentile(p_ms, 50), "p99_ms_per_step": percentile(p_ms, 99),
+                                  "dtype": "f32",
+                                  "path": "FP32 maps, one map per call (vmap_fuse_depth_rgb + vmap_render_scene)"},
+            "ratio_vs_plain": value / p_value, "megapixels_per_step": pixels / 1e6, "dtype": wls[0].voxel_format,
             "hit_fraction_last_step": hits, "error_flags": int(np.bitwise_or.reduce([s["error_flags"] for s in stats])),
             "allocated_blocks_total": int(sum(s["allocated_blocks"] for s in stats))}
 
@@ -456,11 +500,11 @@ def run_product(args):
         vm.release()
     if args.batch > 0:
         wls, desc = batched_same_size(args, wl, rank)
-        line["batched"] = run_batched(args, wls, dev, flush, world, value)
+        line["batched"] = run_batched(args, wls, dev, flush, world)
         line["batched"]["config"] = desc
     if args.uneven > 0:
         wls, desc = batched_uneven(args, rank)
-        line["batched_uneven"] = run_batched(args, wls, dev, flush, world, value, distinct_frames=8)
+        line["batched_uneven"] = run_batched(args, wls, dev, flush, world, distinct_frames=8)
         line["batched_uneven"]["config"] = desc
 
     # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
