@@ -55,6 +55,23 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
+def max_over_ranks(x, device, world):
+    """The maximum of a per-rank number over all ranks (the device time of the
+    slowest rank bounds the job): an all-reduce MAX when world > 1."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(units_per_rank, max_total_ms, world):
+    """Whole-job units per second: every rank processed units_per_rank units
+    within the slowest rank's max_total_ms."""
+    return world * units_per_rank / (max_total_ms / 1e3)
+
+
 def percentile(xs, q):
     return float(np.percentile(np.asarray(xs, np.float64), q)) if xs else 0.0
 
@@ -253,10 +270,7 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
                 ev[k][1].record(side)
             side.synchronize()
         step_ms = [a.elapsed_time(b) for a, b in ev]
-        t = torch.tensor([sum(step_ms)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return step_ms, float(t.item())
+        return step_ms, max_over_ranks(sum(step_ms), dev, world)
 
     # --- batched: one vmap_batch_step over all maps per step
     maps = make_maps(wls)
@@ -276,7 +290,7 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
             f.nmap_dev, f.nmap_pitch = nmaps[b].data_ptr(), w.width * 16
         frames.append(fr)
     step_ms, tot = timed(lambda i: L.check(lib.vmap_batch_step(batch._h, frames[i], sp)))
-    value = world * B * K / (tot / 1e3)
+    value = job_throughput(B * K, tot, world)
     pixels = sum(w.width * w.height for w in wls)
     hits = float(sum(torch.isfinite(v[..., 0]).sum().item() for v in vmaps)) / pixels
     stats = [m.stats() for m in maps]
@@ -299,7 +313,7 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
                                           nmaps[b].data_ptr(), w.width * 16, sp))
 
     p_ms, p_tot = timed(plain_step)
-    p_value = world * B * K / (p_tot / 1e3)
+    p_value = job_throughput(B * K, p_tot, world)
     for m in pmaps:
         m.release()
     return {"value": value, "unit": "frames/s", "maps": B, "steps": K, "warmup": W,
@@ -404,12 +418,10 @@ def run_product(args):
     L.check(lib.vmap_timing_read(h, stage_ms, stage_n))
     L.check(lib.vmap_timing_enable(h, 0))
     total_ms = sum(step_ms)
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    max_total_ms = max_over_ranks(total_ms, dev, world)
     if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
         dist.barrier()
-    max_total_ms = float(t.item())
-    value = world * args.steps / (max_total_ms / 1e3)
+    value = job_throughput(args.steps, max_total_ms, world)
     st = vm.stats()
     cnt = counters.cpu().numpy()
     vis = cnt[:, 1].astype(np.float64)
@@ -460,6 +472,33 @@ def run_product(args):
             "map": {"allocated_blocks": int(st["allocated_blocks"]), "visible_blocks_mean": float(vis.mean()),
                     "error_flags": int(st["error_flags"])}}
 
+    # --- mesh: marching cubes over every allocated block of the map -------
+    # (Polygonize, marching_cubes.cu:251-305): a counting pass, then the emit
+    # pass into buffers of that size; each timed alone after an L2 flush.
+    cnt_d = torch.zeros(1, dtype=torch.int32, device=dev)
+    mev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    flush.fill_(1)
+    mev[0].record()
+    L.check(lib.vmap_polygonize(h, None, None, 0, cnt_d.data_ptr(), sp))
+    mev[1].record()
+    torch.cuda.synchronize()
+    ntri = int(cnt_d.item())
+    mverts = torch.empty((max(ntri, 1), 9), dtype=torch.float32, device=dev)
+    mnorms = torch.empty_like(mverts)
+    flush.fill_(2)
+    mev[2].record()
+    L.check(lib.vmap_polygonize(h, mverts.data_ptr(), mnorms.data_ptr(), ntri, None, sp))
+    mev[3].record()
+    torch.cuda.synchronize()
+    count_ms, emit_ms = mev[0].elapsed_time(mev[1]), mev[2].elapsed_time(mev[3])
+    nblk = float(st["allocated_blocks"])
+    halo = (9.0 / 8.0) ** 3  # a block's 8^3 cubes read a 9^3 voxel neighbourhood
+    mesh_bytes = nblk * 512 * s_tsdf * halo + ntri * 72
+    line["mesh"] = {"triangles": ntri, "blocks": int(nblk), "count_pass_ms": count_ms, "emit_pass_ms": emit_ms,
+                    "alg_bytes_emit": mesh_bytes, "emit_gbs": mesh_bytes / (emit_ms * 1e-3) / 1e9,
+                    "emit_frac_of_peak": mesh_bytes / (emit_ms * 1e-3) / 1e9 / peak}
+    del mverts, mnorms
+
     # --- e2e: same steps through the host-buffer C ABI calls --------------
     if not args.no_e2e:
         depth_h = torch.from_numpy(np.stack([f[0] for f in frames]).view(np.int16)).pin_memory()
@@ -487,10 +526,8 @@ def run_product(args):
             ev2[k][1].record()
         torch.cuda.synchronize()
         e_ms = [a.elapsed_time(b) for a, b in ev2]
-        t2 = torch.tensor([sum(e_ms)], dtype=torch.float64, device=dev)
-        if world > 1:
-            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
-        line["e2e"] = {"value": world * args.steps / (float(t2.item()) / 1e3), "unit": "frames/s",
+        e_tot = max_over_ranks(sum(e_ms), dev, world)
+        line["e2e"] = {"value": job_throughput(args.steps, e_tot, world), "unit": "frames/s",
                        "h2d_bytes_per_step": P * 2 + P * 3, "d2h_bytes_per_step": 2 * P * 16,
                        "p50_ms": percentile(e_ms, 50), "p99_ms": percentile(e_ms, 99),
                        "path": "vmap_fuse_host + vmap_render_scene_host, pinned host buffers"}
