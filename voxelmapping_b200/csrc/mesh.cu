@@ -8,7 +8,8 @@
 // chain walks per cube) and takes one global atomic per triangle. Here a
 // 256-thread CTA stages the block plus its +x/+y/+z halo (9x9x9 voxels, 7
 // neighbour lookups) in shared memory, counts triangles from the packed
-// table, reserves the CTA's output range with one atomic and emits.
+// table, reserves the CTA's output range with one atomic and emits with one
+// thread per triangle.
 #include "vmap_launch.h"
 #include "mc_table.inc"
 
@@ -55,7 +56,9 @@ __global__ void __launch_bounds__(256) mesh_kernel(DevMap m, float* verts, float
     __shared__ unsigned char s_ok[kHalo * kHalo * kHalo];
     __shared__ int s_nb[8];
     __shared__ unsigned s_wsum[8];
-    __shared__ unsigned s_base;
+    __shared__ unsigned s_base, s_total;
+    __shared__ unsigned short s_start[512];  // first triangle of each cube rank within the block
+    __shared__ unsigned char s_ci[512];      // case index of each cube rank
     const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
     s_tab[tid] = kMcTri[tid];
     const int n = allocated_blocks(m);
@@ -119,46 +122,65 @@ __global__ void __launch_bounds__(256) mesh_kernel(DevMap m, float* verts, float
                 run += t;
             }
             s_base = run ? atomicAdd(m.ctr + C_TRI, run) : 0u;
+            s_total = run;
         }
         __syncthreads();
-        if (verts == nullptr || cnt == 0) continue;
-        unsigned t = s_base + s_wsum[wid] + incl - cnt;
-#pragma unroll
-        for (int j = 0; j < 2; ++j) {
-            const unsigned long long code = s_tab[ci[j]];
-            const int ntri = (int)(code >> 60);
-            if (ntri == 0) continue;
-            const int c = tid + 256 * j;
+        if (verts == nullptr) continue;
+        // emission: triangles, not cubes, are spread over the threads, so every
+        // lane writes (a cube-per-thread loop leaves most lanes idle: few cubes
+        // of a block cross the surface). Cube rank r = 2 * tid + j keeps the
+        // scan's order; s_start[r] is its first triangle within the block.
+        {
+            const unsigned first = s_wsum[wid] + incl - cnt;
+            const unsigned n0 = (unsigned)(s_tab[ci[0]] >> 60);
+            s_start[2 * tid] = (unsigned short)first;
+            s_start[2 * tid + 1] = (unsigned short)(first + n0);
+            s_ci[2 * tid] = (unsigned char)ci[0];
+            s_ci[2 * tid + 1] = (unsigned char)ci[1];
+        }
+        __syncthreads();
+        const unsigned total = s_total;
+        for (unsigned q = tid; q < total; q += 256) {
+            const unsigned t = s_base + q;
+            if (t >= maxTris) break;
+            // the last cube rank whose start is <= q (zero-triangle cubes share
+            // their successor's start and precede it)
+            int lo = 0, hi = 511;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (s_start[mid] <= q) lo = mid;
+                else hi = mid - 1;
+            }
+            const int r = lo, k = (int)(q - s_start[r]);
+            const int c = (r >> 1) + 256 * (r & 1);
+            const unsigned long long code = s_tab[s_ci[r]];
             const int x = c & 7, y = (c >> 3) & 7, z = c >> 6;
             const int e0 = (z * kHalo + y) * kHalo + x;
             const float s[8] = {s_sdf[e0], s_sdf[e0 + 1], s_sdf[e0 + kHalo + 1], s_sdf[e0 + kHalo],
                                 s_sdf[e0 + 81], s_sdf[e0 + 82], s_sdf[e0 + 81 + kHalo + 1], s_sdf[e0 + 81 + kHalo]};
             const float fbx = __int2float_rn(bp.x * 8 + x), fby = __int2float_rn(bp.y * 8 + y),
                         fbz = __int2float_rn(bp.z * 8 + z);
-            for (int k = 0; k < ntri; ++k, ++t) {
-                if (t >= maxTris) continue;
-                const int ea = (int)((code >> (12 * k)) & 15), eb = (int)((code >> (12 * k + 4)) & 15),
-                          ec = (int)((code >> (12 * k + 8)) & 15);
-                // reversed winding: tri[2] = v[a], tri[1] = v[b], tri[0] = v[c], all * voxel size
-                const float3 va = edge_vertex(ea, s, fbx, fby, fbz), vb = edge_vertex(eb, s, fbx, fby, fbz),
-                             vc = edge_vertex(ec, s, fbx, fby, fbz);
-                const float3 t2 = make_float3(__fmul_rn(va.x, m.vs), __fmul_rn(va.y, m.vs), __fmul_rn(va.z, m.vs));
-                const float3 t1 = make_float3(__fmul_rn(vb.x, m.vs), __fmul_rn(vb.y, m.vs), __fmul_rn(vb.z, m.vs));
-                const float3 t0 = make_float3(__fmul_rn(vc.x, m.vs), __fmul_rn(vc.y, m.vs), __fmul_rn(vc.z, m.vs));
-                const float3 nrm = normalized(cross3(make_float3(__fsub_rn(t1.x, t0.x), __fsub_rn(t1.y, t0.y), __fsub_rn(t1.z, t0.z)),
-                                                     make_float3(__fsub_rn(t2.x, t0.x), __fsub_rn(t2.y, t0.y), __fsub_rn(t2.z, t0.z))));
-                float* vo = verts + 9 * (size_t)t;
-                vo[0] = t0.x; vo[1] = t0.y; vo[2] = t0.z;
-                vo[3] = t1.x; vo[4] = t1.y; vo[5] = t1.z;
-                vo[6] = t2.x; vo[7] = t2.y; vo[8] = t2.z;
-                if (norms) {
-                    float* no = norms + 9 * (size_t)t;
+            const int ea = (int)((code >> (12 * k)) & 15), eb = (int)((code >> (12 * k + 4)) & 15),
+                      ec = (int)((code >> (12 * k + 8)) & 15);
+            // reversed winding: tri[2] = v[a], tri[1] = v[b], tri[0] = v[c], all * voxel size
+            const float3 va = edge_vertex(ea, s, fbx, fby, fbz), vb = edge_vertex(eb, s, fbx, fby, fbz),
+                         vc = edge_vertex(ec, s, fbx, fby, fbz);
+            const float3 t2 = make_float3(__fmul_rn(va.x, m.vs), __fmul_rn(va.y, m.vs), __fmul_rn(va.z, m.vs));
+            const float3 t1 = make_float3(__fmul_rn(vb.x, m.vs), __fmul_rn(vb.y, m.vs), __fmul_rn(vb.z, m.vs));
+            const float3 t0 = make_float3(__fmul_rn(vc.x, m.vs), __fmul_rn(vc.y, m.vs), __fmul_rn(vc.z, m.vs));
+            const float3 nrm = normalized(cross3(make_float3(__fsub_rn(t1.x, t0.x), __fsub_rn(t1.y, t0.y), __fsub_rn(t1.z, t0.z)),
+                                                 make_float3(__fsub_rn(t2.x, t0.x), __fsub_rn(t2.y, t0.y), __fsub_rn(t2.z, t0.z))));
+            float* vo = verts + 9 * (size_t)t;
+            vo[0] = t0.x; vo[1] = t0.y; vo[2] = t0.z;
+            vo[3] = t1.x; vo[4] = t1.y; vo[5] = t1.z;
+            vo[6] = t2.x; vo[7] = t2.y; vo[8] = t2.z;
+            if (norms) {
+                float* no = norms + 9 * (size_t)t;
 #pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        no[3 * q] = nrm.x;
-                        no[3 * q + 1] = nrm.y;
-                        no[3 * q + 2] = nrm.z;
-                    }
+                for (int w = 0; w < 3; ++w) {
+                    no[3 * w] = nrm.x;
+                    no[3 * w + 1] = nrm.y;
+                    no[3 * w + 2] = nrm.z;
                 }
             }
         }
