@@ -48,6 +48,8 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=0, help="timed batched steps (default: --steps // 4)")
     p.add_argument("--batch-blocks", type=int, default=1 << 17, help="block pool per batched map")
     p.add_argument("--uneven", type=int, default=64, help="maps of the uneven batch (0 skips it)")
+    p.add_argument("--autotune", action="store_true",
+                   help="tune the launch shapes first (else a cached or shipped table, if any, is applied)")
     return p.parse_args()
 
 
@@ -70,6 +72,23 @@ def job_throughput(units_per_rank, max_total_ms, world):
     """Whole-job units per second: every rank processed units_per_rank units
     within the slowest rank's max_total_ms."""
     return world * units_per_rank / (max_total_ms / 1e3)
+
+
+def apply_tuning(target, key, args, tune):
+    """Launch shapes for `target` (a map or batch): tuned now with --autotune
+    (and cached), else the cached or shipped entry for `key`, else defaults.
+    Returns (config, source)."""
+    from voxelmapping_b200 import autotune as AT
+    if args.autotune and tune is not None:
+        cfg, table = tune()
+        AT.store(key, cfg, {"medians_ms": {f: {str(c): v for c, v in t.items()} for f, t in table.items()}})
+        target.set_launch_config(**cfg)
+        return cfg, "tuned"
+    cfg, src = AT.lookup(key)
+    if cfg:
+        target.set_launch_config(**cfg)
+        return cfg, src
+    return target.get_launch_config(), "default"
 
 
 def percentile(xs, q):
@@ -289,7 +308,24 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
             f.vmap_dev, f.vmap_pitch = vmaps[b].data_ptr(), w.width * 16
             f.nmap_dev, f.nmap_pitch = nmaps[b].data_ptr(), w.width * 16
         frames.append(fr)
-    step_ms, tot = timed(lambda i: L.check(lib.vmap_batch_step(batch._h, frames[i], sp)))
+    def batch_step(i):
+        L.check(lib.vmap_batch_step(batch._h, frames[i % nfr], sp))
+    batch_step.stream = side
+
+    def tune():
+        from voxelmapping_b200 import autotune as AT
+        torch.cuda.synchronize()
+        res = AT.tune_batch(batch, batch_step)
+        torch.cuda.synchronize()
+        for m in maps:  # the timed steps start from empty maps
+            m.reset()
+        torch.cuda.synchronize()
+        return res
+    from voxelmapping_b200 import autotune as AT
+    key = AT.key_for("batch", wls[0].voxel_format, wls[0].width, wls[0].height, B) if len(
+        {(w.width, w.height) for w in wls}) == 1 else AT.key_for("batch", wls[0].voxel_format, 0, 0, B)
+    launch_cfg, tune_src = apply_tuning(batch, key, args, tune)
+    step_ms, tot = timed(batch_step)
     value = job_throughput(B * K, tot, world)
     pixels = sum(w.width * w.height for w in wls)
     hits = float(sum(torch.isfinite(v[..., 0]).sum().item() for v in vmaps)) / pixels
@@ -301,6 +337,11 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
     # --- plain: the same frames, FP32 maps, one map per call
     pwls = [dataclasses.replace(w, voxel_format="f32", max_weight=255) for w in wls]
     pmaps = make_maps(pwls)
+    from voxelmapping_b200 import autotune as AT
+    for w, m in zip(pwls, pmaps):  # the plain path with its own tuned shapes, where a table has them
+        cfg, _ = AT.lookup(AT.key_for("map", w.voxel_format, w.width, w.height))
+        if cfg:
+            m.set_launch_config(**cfg)
     pargs = [[L.pose_arg(poses[b][j].reshape(4, 4)) for j in range(F)] for b in range(B)]
 
     def plain_step(i):
@@ -324,6 +365,7 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
                                   "dtype": "f32",
                                   "path": "FP32 maps, one map per call (vmap_fuse_depth_rgb + vmap_render_scene)"},
             "ratio_vs_plain": value / p_value, "megapixels_per_step": pixels / 1e6, "dtype": wls[0].voxel_format,
+            "launch_config": launch_cfg, "tuning": tune_src,
             "hit_fraction_last_step": hits, "error_flags": int(np.bitwise_or.reduce([s["error_flags"] for s in stats])),
             "allocated_blocks_total": int(sum(s["allocated_blocks"] for s in stats))}
 
@@ -395,6 +437,26 @@ def run_product(args):
         L.check(lib.vmap_fuse_depth_rgb(h, depth_d[i].data_ptr(), L.DEPTH_U16, wl.width * 2, wl.depth_scale,
                                         rgb_d[i].data_ptr(), wl.width * 3, poses[i], sp))
         L.check(lib.vmap_render_scene(h, poses[i], vmap.data_ptr(), vpitch, nmap.data_ptr(), vpitch, sp))
+
+    def tune():
+        # on a scratch map of the same configuration, so the timed map's
+        # frames and state stay those of the measured workload
+        from voxelmapping_b200 import autotune as AT
+        tmp = VoxelMapping(wl.width, wl.height, wl.K, voxel_format=wl.voxel_format, with_color=wl.with_color,
+                           max_weight=wl.max_weight)
+        tmp.CreateMap(wl.num_entries, wl.num_blocks, wl.voxel_size)
+
+        def tstep(i):
+            j = i % nfr
+            L.check(lib.vmap_fuse_depth_rgb(tmp._map, depth_d[j].data_ptr(), L.DEPTH_U16, wl.width * 2,
+                                            wl.depth_scale, rgb_d[j].data_ptr(), wl.width * 3, poses[j], sp))
+            L.check(lib.vmap_render_scene(tmp._map, poses[j], vmap.data_ptr(), vpitch, nmap.data_ptr(), vpitch, sp))
+        best, table = AT.tune_map(tmp, tstep, n_steps=8)
+        best["mesh_ctas_per_sm"], table["mesh_ctas_per_sm"] = AT.tune_mesh(tmp)
+        tmp.release()
+        return best, table
+    from voxelmapping_b200 import autotune as AT
+    launch_cfg, tune_src = apply_tuning(vm, AT.key_for("map", wl.voxel_format, wl.width, wl.height), args, tune)
 
     for i in range(args.warmup):
         step(i)
@@ -469,6 +531,7 @@ def run_product(args):
             "scaling": "weak", "vs_baseline": None, "dtype": wl.voxel_format, "data": "synthetic",
             "config": workload_config(wl, args), "roofline": roof, "stages": stages,
             "gpu_launches": int(sum(stage_n)), "clocks": clk.summary(),
+            "launch_config": launch_cfg, "tuning": tune_src,
             "map": {"allocated_blocks": int(st["allocated_blocks"]), "visible_blocks_mean": float(vis.mean()),
                     "error_flags": int(st["error_flags"])}}
 

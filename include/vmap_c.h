@@ -226,6 +226,27 @@ vmap_status vmap_batch_destroy(vmap_batch* batch);
  * step before last has copied its descriptors. */
 vmap_status vmap_batch_step(vmap_batch* batch, const vmap_batch_frame* frames, void* stream);
 
+/* ---- launch shapes (no counterpart in the reference, which hard-codes its
+ * grids). Every stage's grid in CTAs per SM; each kernel strides over its work
+ * items, so any shape gives the same results and only the time changes.
+ * 0 in a field selects the library default (alloc 8, visibility 2, fuse 16,
+ * zrange 4, normals 8, mesh 8; raycast 0 = as many CTAs as fit on an SM, the
+ * ray marcher being persistent). Values above 64 are refused. Setting a
+ * batch's shapes synchronises the device and records its graphs again. */
+typedef struct vmap_launch_config {
+    int alloc_ctas_per_sm;
+    int visibility_ctas_per_sm;
+    int fuse_ctas_per_sm;
+    int zrange_ctas_per_sm;
+    int raycast_ctas_per_sm;
+    int normals_ctas_per_sm;
+    int mesh_ctas_per_sm;
+} vmap_launch_config;
+vmap_status vmap_get_launch_config(const vmap_map* map, vmap_launch_config* out);
+vmap_status vmap_set_launch_config(vmap_map* map, const vmap_launch_config* cfg);
+vmap_status vmap_batch_get_launch_config(const vmap_batch* batch, vmap_launch_config* out);
+vmap_status vmap_batch_set_launch_config(vmap_batch* batch, const vmap_launch_config* cfg);
+
 /* ---- inspection ---------------------------------------------------------- */
 /* Synchronises `stream`, then reads the device counters. */
 vmap_status vmap_get_stats(vmap_map* map, void* stream, vmap_stats* out);

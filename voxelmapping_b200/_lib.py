@@ -53,6 +53,13 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class LaunchConfig(C.Structure):
+    """vmap_launch_config: grid of every stage in CTAs per SM (0 = default)."""
+    _fields_ = [("alloc_ctas_per_sm", C.c_int), ("visibility_ctas_per_sm", C.c_int), ("fuse_ctas_per_sm", C.c_int),
+                ("zrange_ctas_per_sm", C.c_int), ("raycast_ctas_per_sm", C.c_int), ("normals_ctas_per_sm", C.c_int),
+                ("mesh_ctas_per_sm", C.c_int)]
+
+
 class BatchFrame(C.Structure):
     _fields_ = [("depth_dev", C.c_void_p), ("depth_type", C.c_int), ("depth_pitch", C.c_size_t),
                 ("depth_scale", C.c_float), ("rgb_dev", C.c_void_p), ("rgb_pitch", C.c_size_t),
@@ -94,6 +101,10 @@ SIGNATURES = {
     "vmap_create_in": (C.c_int, [C.POINTER(Config), P, C.c_uint64, P, C.POINTER(P)]),
     "vmap_batch_create_slots": (C.c_int, [C.c_int, C.c_int, C.POINTER(P)]),
     "vmap_batch_set_map": (C.c_int, [P, C.c_int, P]),
+    "vmap_get_launch_config": (C.c_int, [P, C.POINTER(LaunchConfig)]),
+    "vmap_set_launch_config": (C.c_int, [P, C.POINTER(LaunchConfig)]),
+    "vmap_batch_get_launch_config": (C.c_int, [P, C.POINTER(LaunchConfig)]),
+    "vmap_batch_set_launch_config": (C.c_int, [P, C.POINTER(LaunchConfig)]),
     "vmap_snapshot_save": (C.c_int, [P, P, C.c_uint64, C.POINTER(C.c_uint64), P]),
     "vmap_snapshot_load": (C.c_int, [P, P, C.c_uint64, P]),
     "vmap_timing_enable": (C.c_int, [P, C.c_uint32]),

@@ -1,0 +1,188 @@
+"""Launch-shape autotuner for the fuse / raycast / mesh stages.
+
+The library's kernels stride over their work items, so a stage's grid (CTAs
+per SM, vmap_launch_config) changes only its time. The tuner measures the
+candidates on the caller's own data and keeps the fastest:
+
+* a single map (`tune_map`): every trial sets every stage to one candidate and
+  reads the per-stage CUDA-event times (vmap_timing_*), so all stages are
+  tuned together; candidates are visited round-robin several times and each
+  keeps its median;
+* a batch (`tune_batch`): the stages run inside one recorded CUDA graph, so
+  the whole step is timed, one stage at a time (coordinate descent);
+* the mesh grid (`tune_mesh`): the counting pass of vmap_polygonize.
+
+Results are cached as JSON keyed by device name, path (map or batch), voxel
+format and image size: in $VMAP_TUNING_CACHE, else
+~/.cache/voxelmapping_b200/tuning.json. `tuning_b200.json` beside this file
+holds a table measured on a B200, used when the cache has no entry.
+"""
+import ctypes as C
+import json
+import os
+import statistics
+from pathlib import Path
+
+from . import _lib as L
+
+FIELDS = ["alloc_ctas_per_sm", "visibility_ctas_per_sm", "fuse_ctas_per_sm", "zrange_ctas_per_sm",
+          "raycast_ctas_per_sm", "normals_ctas_per_sm", "mesh_ctas_per_sm"]
+STAGE = {"alloc_ctas_per_sm": "alloc", "visibility_ctas_per_sm": "visibility", "fuse_ctas_per_sm": "fuse",
+         "zrange_ctas_per_sm": "zrange", "raycast_ctas_per_sm": "raycast", "normals_ctas_per_sm": "normals"}
+CANDIDATES = {
+    "alloc_ctas_per_sm": [2, 4, 8, 16],
+    "visibility_ctas_per_sm": [1, 2, 4, 8],
+    "fuse_ctas_per_sm": [4, 8, 16, 32],
+    "zrange_ctas_per_sm": [1, 2, 4, 8],
+    "raycast_ctas_per_sm": [2, 3, 4, 0],
+    "normals_ctas_per_sm": [2, 4, 8, 16],
+    "mesh_ctas_per_sm": [4, 8, 16, 32],
+}
+SHIPPED = Path(__file__).resolve().parent / "tuning_b200.json"
+
+
+def cache_path():
+    p = os.environ.get("VMAP_TUNING_CACHE")
+    return Path(p) if p else Path.home() / ".cache" / "voxelmapping_b200" / "tuning.json"
+
+
+def device_name():
+    import torch
+    if not torch.cuda.is_available():
+        return "no-cuda-device"
+    return torch.cuda.get_device_name(torch.cuda.current_device())
+
+
+def key_for(kind, voxel_format, width, height, n_maps=1):
+    """kind: "map" or "batch" (batches are keyed by their map count too; a
+    batch of maps of different sizes uses width = height = 0)."""
+    k = "%s|%s|%s|%dx%d" % (device_name(), kind, voxel_format, width, height)
+    if kind == "batch":
+        k += "|maps=%d" % n_maps
+    return k
+
+
+def _read(path):
+    try:
+        return json.loads(Path(path).read_text())
+    except (OSError, ValueError):
+        return {}
+
+
+def lookup(key):
+    """(launch config dict, source) of the cached or shipped entry, or (None, None)."""
+    for src, path in (("cache", cache_path()), ("shipped", SHIPPED)):
+        entry = _read(path).get(key)
+        if entry:
+            return {f: int(entry["config"].get(f, 0)) for f in FIELDS}, src
+    return None, None
+
+
+def store(key, config, meta=None):
+    path = cache_path()
+    path.parent.mkdir(parents=True, exist_ok=True)
+    table = _read(path)
+    table[key] = {"config": config, "meta": meta or {}}
+    tmp = path.with_suffix(".tmp")
+    tmp.write_text(json.dumps(table, indent=1, sort_keys=True))
+    tmp.replace(path)
+
+
+def tune_map(vm, step, n_steps, rounds=3, warmup=3):
+    """Tunes a single map's stage grids. step(i) runs step i (fuse + render)
+    on the current stream. Returns (best config, {field: {candidate: median ms}})."""
+    import torch
+    lib = L.lib()
+    base = vm.get_launch_config()
+    for i in range(warmup):
+        step(i)
+    torch.cuda.synchronize()
+    n_cand = max(len(CANDIDATES[f]) for f in STAGE)
+    samples = {f: {c: [] for c in CANDIDATES[f]} for f in STAGE}
+    it = warmup
+    for _ in range(rounds):
+        for t in range(n_cand):
+            cfg = dict(base)
+            for f in STAGE:
+                cfg[f] = CANDIDATES[f][t % len(CANDIDATES[f])]
+            vm.set_launch_config(**cfg)
+            L.check(lib.vmap_timing_enable(vm._map, 8 * n_steps))
+            for _ in range(n_steps):
+                step(it)
+                it += 1
+            torch.cuda.synchronize()
+            ms = (C.c_double * 7)()
+            cnt = (C.c_uint32 * 7)()
+            L.check(lib.vmap_timing_read(vm._map, ms, cnt))
+            L.check(lib.vmap_timing_enable(vm._map, 0))
+            for f, stage in STAGE.items():
+                i = L.STAGES.index(stage)
+                if cnt[i]:
+                    samples[f][cfg[f]].append(ms[i] / cnt[i])
+    best = dict(base)
+    table = {}
+    for f in STAGE:
+        med = {c: statistics.median(v) for c, v in samples[f].items() if v}
+        if med:  # a stage the step never runs (a render without normals) keeps its shape
+            table[f] = med
+            best[f] = min(med, key=med.get)
+    vm.set_launch_config(**best)
+    return best, table
+
+
+def tune_mesh(vm, rounds=3):
+    """Tunes the marching-cubes grid on the counting pass. Returns (best, {candidate: median ms})."""
+    import torch
+    lib = L.lib()
+    cnt = torch.zeros(1, dtype=torch.int32, device="cuda")
+    s = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    L.check(lib.vmap_polygonize(vm._map, None, None, 0, C.c_void_p(cnt.data_ptr()), s))  # loads the kernels
+    samples = {c: [] for c in CANDIDATES["mesh_ctas_per_sm"]}
+    for _ in range(rounds):
+        for c in samples:
+            vm.set_launch_config(mesh_ctas_per_sm=c)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            L.check(lib.vmap_polygonize(vm._map, None, None, 0, C.c_void_p(cnt.data_ptr()), s))
+            b.record()
+            torch.cuda.synchronize()
+            samples[c].append(a.elapsed_time(b))
+    med = {c: statistics.median(v) for c, v in samples.items()}
+    best = min(med, key=med.get)
+    vm.set_launch_config(mesh_ctas_per_sm=best)
+    return best, med
+
+
+def tune_batch(batch, step, n_steps=4, rounds=2, fields=None):
+    """Coordinate descent over the batch's stage grids on whole-step time.
+    step(i) runs batch step i on a non-default stream `step.stream`. Returns
+    (best config, {field: {candidate: median ms per step}})."""
+    import torch
+    stream = step.stream
+    best = batch.get_launch_config()
+    table = {}
+    it = 0
+    for f in fields or [f for f in FIELDS if f != "mesh_ctas_per_sm"]:
+        samples = {c: [] for c in CANDIDATES[f]}
+        for _ in range(rounds):
+            for c in samples:
+                cfg = dict(best)
+                cfg[f] = c
+                batch.set_launch_config(**cfg)
+                with torch.cuda.stream(stream):
+                    for _ in range(2):  # the first two steps record the graphs
+                        step(it)
+                        it += 1
+                    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                    a.record(stream)
+                    for _ in range(n_steps):
+                        step(it)
+                        it += 1
+                    b.record(stream)
+                stream.synchronize()
+                samples[c].append(a.elapsed_time(b) / n_steps)
+        med = {c: statistics.median(v) for c, v in samples.items()}
+        table[f] = med
+        best[f] = min(med, key=med.get)
+    batch.set_launch_config(**best)
+    return best, table

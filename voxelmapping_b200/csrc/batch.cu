@@ -184,6 +184,27 @@ vmap_status vmap_batch_set_map(vmap_batch* b, int slot, vmap_map* map)
     return VMAP_OK;
 }
 
+vmap_status vmap_batch_get_launch_config(const vmap_batch* b, vmap_launch_config* out)
+{
+    if (!b || !out) return VMAP_ERR_INVALID_ARG;
+    launch_config_from(b->launcher, out);
+    return VMAP_OK;
+}
+
+vmap_status vmap_batch_set_launch_config(vmap_batch* b, const vmap_launch_config* cfg)
+{
+    if (!b || !cfg || !launch_config_ok(cfg)) return VMAP_ERR_INVALID_ARG;
+    // the recorded graphs hold the old grids: record again once the steps in flight are done
+    VMAP_BCK(cudaDeviceSynchronize());
+    for (int i = 0; i < 2; ++i)
+        if (b->exec[i]) {
+            cudaGraphExecDestroy(b->exec[i]);
+            b->exec[i] = nullptr;
+        }
+    launch_config_to(cfg, b->launcher);
+    return VMAP_OK;
+}
+
 vmap_status vmap_batch_destroy(vmap_batch* b)
 {
     if (!b) return VMAP_ERR_INVALID_ARG;

@@ -286,22 +286,21 @@ __global__ void reset_hash_kernel(DevMap m)
 template <class V>
 cudaError_t launch_alloc(const V& views, int totalTiles, const Launcher& l, cudaStream_t s)
 {
-    const int grid = totalTiles < l.numSMs * 8 ? (totalTiles > 0 ? totalTiles : 1) : l.numSMs * 8;
-    alloc_kernel<V><<<grid, 256, 0, s>>>(views);
+    alloc_kernel<V><<<stage_grid(l, l.alloc, totalTiles), 256, 0, s>>>(views);
     return cudaGetLastError();
 }
 
 template <class V>
 cudaError_t launch_visibility(const V& views, const Launcher& l, cudaStream_t s)
 {
-    visibility_kernel<V><<<l.numSMs * 2, 256, 0, s>>>(views);
+    visibility_kernel<V><<<stage_grid(l, l.visibility), 256, 0, s>>>(views);
     return cudaGetLastError();
 }
 
 template <class V>
 cudaError_t launch_fuse(const V& views, int fmt, const Launcher& l, cudaStream_t s)
 {
-    const int grid = l.numSMs * 16;
+    const int grid = stage_grid(l, l.fuse);
     switch (fmt) {
     case VMAP_VOXEL_REF: fuse_kernel<V, VMAP_VOXEL_REF><<<grid, 256, 0, s>>>(views); break;
     case VMAP_VOXEL_F32: fuse_kernel<V, VMAP_VOXEL_F32><<<grid, 256, 0, s>>>(views); break;

@@ -368,6 +368,7 @@ vmap_status build_map(const vmap_config& cfg, unsigned char* base, cudaStream_t 
     m->cfg = cfg;
     m->device = dev;
     m->external = base != nullptr;
+    m->launcher = Launcher();  // the memset above cleared the default grid shapes
     m->launcher.numSMs = sms;
     m->tilesX = (cfg.width + kZTile - 1) / kZTile;
     m->tilesY = (cfg.height + kZTile - 1) / kZTile;
@@ -460,6 +461,20 @@ vmap_status vmap_destroy(vmap_map* m)
     if (!m->external) cudaDeviceSynchronize();
     free_all(m);
     delete m;
+    return VMAP_OK;
+}
+
+vmap_status vmap_get_launch_config(const vmap_map* m, vmap_launch_config* out)
+{
+    if (!m || !out) return VMAP_ERR_INVALID_ARG;
+    launch_config_from(m->launcher, out);
+    return VMAP_OK;
+}
+
+vmap_status vmap_set_launch_config(vmap_map* m, const vmap_launch_config* cfg)
+{
+    if (!m || !cfg || !launch_config_ok(cfg)) return VMAP_ERR_INVALID_ARG;
+    launch_config_to(cfg, m->launcher);
     return VMAP_OK;
 }
 
@@ -614,7 +629,8 @@ vmap_status vmap_compute_normal(const float* vmap_dev, size_t vmap_pitch, float*
     int dev = 0, sms = 1;
     VMAP_CK(cudaGetDevice(&dev));
     VMAP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    Launcher l{sms};
+    Launcher l;
+    l.numSMs = sms;
     VMAP_CK(launch_normals(ov, tiles_32x8(width, height), l, as_stream(stream)));
     return VMAP_OK;
 }

@@ -241,7 +241,7 @@ cudaError_t launch_mesh(const DevMap& m, int fmt, float* verts, float* norms, un
 {
     cudaError_t e = cudaMemsetAsync(m.ctr + C_TRI, 0, sizeof(unsigned), s);
     if (e != cudaSuccess) return e;
-    const int grid = l.numSMs * 8;
+    const int grid = stage_grid(l, l.mesh);
     switch (fmt) {
     case VMAP_VOXEL_REF: mesh_kernel<VMAP_VOXEL_REF><<<grid, 256, 0, s>>>(m, verts, norms, maxTris); break;
     case VMAP_VOXEL_F32: mesh_kernel<VMAP_VOXEL_F32><<<grid, 256, 0, s>>>(m, verts, norms, maxTris); break;

@@ -182,15 +182,14 @@ __global__ void __launch_bounds__(256) phong_kernel(const float4* vmap, size_t v
 template <class V>
 cudaError_t launch_zrange(const V& views, const Launcher& l, cudaStream_t s)
 {
-    zrange_kernel<V><<<l.numSMs * 4, 256, 0, s>>>(views);
+    zrange_kernel<V><<<stage_grid(l, l.zrange), 256, 0, s>>>(views);
     return cudaGetLastError();
 }
 
 template <class V>
 cudaError_t launch_normals(const V& views, int totalTiles, const Launcher& l, cudaStream_t s)
 {
-    const int grid = totalTiles < l.numSMs * 8 ? (totalTiles > 0 ? totalTiles : 1) : l.numSMs * 8;
-    normals_kernel<V><<<grid, 256, 0, s>>>(views);
+    normals_kernel<V><<<stage_grid(l, l.normals, totalTiles), 256, 0, s>>>(views);
     return cudaGetLastError();
 }
 

@@ -433,7 +433,9 @@ static cudaError_t raycast_persistent(const V& views, const Launcher& l, cudaStr
         cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, raycast_kernel<V, FMT>, 256, 0);
         if (e != cudaSuccess || occ < 1) occ = 1;
     }
-    raycast_kernel<V, FMT><<<l.numSMs * occ, 256, 0, s>>>(views);
+    // CTAs beyond those resident would only start once others finish: cap at occupancy
+    const int per_sm = l.raycast > 0 && l.raycast < occ ? l.raycast : occ;
+    raycast_kernel<V, FMT><<<stage_grid(l, per_sm), 256, 0, s>>>(views);
     return cudaGetLastError();
 }
 

@@ -16,9 +16,56 @@ struct vmap_map;
 
 namespace vmapb {
 
+// Grid shape of every stage, in CTAs per SM (vmap_launch_config). Each kernel
+// strides over its work items, so any grid gives the same result; the
+// defaults are measured choices, the autotuner may pick others.
 struct Launcher {
     int numSMs;
+    int alloc = 8, visibility = 2, fuse = 16, zrange = 4;
+    int raycast = 0;  // persistent ray marcher: 0 = as many CTAs as fit on an SM
+    int normals = 8, mesh = 8;
 };
+
+// vmap_launch_config <-> Launcher (0 in a field: the default)
+inline bool launch_config_ok(const vmap_launch_config* c)
+{
+    const int v[7] = {c->alloc_ctas_per_sm, c->visibility_ctas_per_sm, c->fuse_ctas_per_sm, c->zrange_ctas_per_sm,
+                      c->raycast_ctas_per_sm, c->normals_ctas_per_sm, c->mesh_ctas_per_sm};
+    for (int x : v)
+        if (x < 0 || x > 64) return false;
+    return true;
+}
+
+inline void launch_config_to(const vmap_launch_config* c, Launcher& l)
+{
+    const Launcher d = Launcher();
+    l.alloc = c->alloc_ctas_per_sm ? c->alloc_ctas_per_sm : d.alloc;
+    l.visibility = c->visibility_ctas_per_sm ? c->visibility_ctas_per_sm : d.visibility;
+    l.fuse = c->fuse_ctas_per_sm ? c->fuse_ctas_per_sm : d.fuse;
+    l.zrange = c->zrange_ctas_per_sm ? c->zrange_ctas_per_sm : d.zrange;
+    l.raycast = c->raycast_ctas_per_sm;
+    l.normals = c->normals_ctas_per_sm ? c->normals_ctas_per_sm : d.normals;
+    l.mesh = c->mesh_ctas_per_sm ? c->mesh_ctas_per_sm : d.mesh;
+}
+
+inline void launch_config_from(const Launcher& l, vmap_launch_config* c)
+{
+    c->alloc_ctas_per_sm = l.alloc;
+    c->visibility_ctas_per_sm = l.visibility;
+    c->fuse_ctas_per_sm = l.fuse;
+    c->zrange_ctas_per_sm = l.zrange;
+    c->raycast_ctas_per_sm = l.raycast;
+    c->normals_ctas_per_sm = l.normals;
+    c->mesh_ctas_per_sm = l.mesh;
+}
+
+// grid of `per_sm` CTAs per SM, or fewer when there are fewer work items
+inline int stage_grid(const Launcher& l, int per_sm, long long items = -1)
+{
+    const long long g = (long long)l.numSMs * per_sm;
+    if (items >= 0 && items < g) return items > 0 ? (int)items : 1;
+    return (int)g;
+}
 
 // fusion.cu
 template <class V>

@@ -104,6 +104,19 @@ class VoxelMapping:
             raise L.VmapError(1, "map not created (call CreateMap first)")
         return self._map
 
+    def get_launch_config(self):
+        """Grid of every stage in CTAs per SM (vmap_get_launch_config)."""
+        c = L.LaunchConfig()
+        L.check(self._lib.vmap_get_launch_config(self._need(), C.byref(c)), "vmap_get_launch_config")
+        return {k: getattr(c, k) for k, _ in c._fields_}
+
+    def set_launch_config(self, **kw):
+        """Sets some stages' grids (keys of get_launch_config; 0 = default)."""
+        cur = self.get_launch_config()
+        cur.update(kw)
+        L.check(self._lib.vmap_set_launch_config(self._need(), C.byref(L.LaunchConfig(**cur))),
+                "vmap_set_launch_config")
+
     def get_config(self):
         cfg = L.Config()
         L.check(self._lib.vmap_get_config(self._need(), C.byref(cfg)), "vmap_get_config")
@@ -268,6 +281,18 @@ class MapBatch:
         L.check(self._lib.vmap_batch_create(arr, len(self.maps), C.byref(h)), "vmap_batch_create")
         self._h = h
         self._frames = (L.BatchFrame * len(self.maps))()
+
+    def get_launch_config(self):
+        c = L.LaunchConfig()
+        L.check(self._lib.vmap_batch_get_launch_config(self._h, C.byref(c)), "vmap_batch_get_launch_config")
+        return {k: getattr(c, k) for k, _ in c._fields_}
+
+    def set_launch_config(self, **kw):
+        """Sets some stages' grids; the batch records its graphs again."""
+        cur = self.get_launch_config()
+        cur.update(kw)
+        L.check(self._lib.vmap_batch_set_launch_config(self._h, C.byref(L.LaunchConfig(**cur))),
+                "vmap_batch_set_launch_config")
 
     def release(self):
         if getattr(self, "_h", None) is not None:
