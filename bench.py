@@ -48,6 +48,11 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=0, help="timed batched steps (default: --steps // 4)")
     p.add_argument("--batch-blocks", type=int, default=1 << 17, help="block pool per batched map")
     p.add_argument("--uneven", type=int, default=64, help="maps of the uneven batch (0 skips it)")
+    p.add_argument("--serving", action="store_true",
+                   help="also run the serving sweep (256 sessions, Poisson arrivals, 70/25/5 fuse/raycast/mesh)")
+    p.add_argument("--serving-rates", default="100,200,300,400,600")
+    p.add_argument("--serving-budgets", default="1.0,0.5", help="device memory budgets, fractions of all sessions' bytes")
+    p.add_argument("--serving-requests", type=int, default=1500)
     p.add_argument("--autotune", action="store_true",
                    help="tune the launch shapes first (else a cached or shipped table, if any, is applied)")
     return p.parse_args()
@@ -616,6 +621,21 @@ def run_product(args):
                                 "kind": "port",
                                 "sample": "frames 0..%d of %s (fuse + raycast each, FP32 reference-algorithm "
                                           "restatement, %d threads)" % (len(times) - 1, WORKLOAD, threads)}
+    if args.serving:
+        from voxelmapping_b200 import serving as S
+        rates = [float(r) for r in args.serving_rates.split(",")]
+        line["serving"] = {"config": "256 sessions of uneven extent / voxel size / resolution (FP16 + colour), 4 "
+                                     "pre-rendered frames each in pinned host memory; Poisson arrivals at each offered "
+                                     "rate, %d requests, 70/25/5 fuse/raycast/mesh; raycasts return vertex + normal "
+                                     "maps to pinned host memory, meshes their triangles; latency = completion - "
+                                     "arrival, wall clock" % args.serving_requests, "runs": []}
+        for frac in [float(b) for b in args.serving_budgets.split(",")]:
+            res, ex = S.run_serving(n_sessions=256, rates=rates, count=args.serving_requests, budget_frac=frac,
+                                    warmup=500, seed=rank)
+            ex.release()
+            for r in res:
+                r["budget_frac"] = frac
+                line["serving"]["runs"].append({k: v for k, v in r.items() if not k.startswith("_")})
     if rank == 0:
         print(json.dumps(line), flush=True)
     vm.release()

@@ -251,8 +251,8 @@ class GpuExecutor:
         with torch.cuda.stream(self.stream):
             n = vm.snapshot_bytes()
             buf = self.snaps.get(s)
-            if buf is None or buf.numel() < n:
-                buf = torch.empty(max(n, 1 << 16) * 5 // 4, dtype=torch.uint8, pin_memory=True)
+            if buf is None or buf.numel() < n:  # room to grow: pinning host memory is slow
+                buf = torch.empty(max(2 * n, 16 << 20), dtype=torch.uint8, pin_memory=True)
             self.snaps[s] = buf[:vm.save_snapshot(buf).shape[0]]  # synchronous
         L.check(self.lib.vmap_batch_set_map(self.batch, slot, None), "vmap_batch_set_map")
         vm.release()  # the map's memory returns to torch's cache; nothing of it is in flight
@@ -439,7 +439,8 @@ def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, 
                 seed=0, warmup=500, max_mesh_per_tick=2, keep_results=False, pool_scale=1, log=None):
     """Builds n_sessions uneven sessions (FP16 + colour), then for each rate
     replays `count` Poisson requests (70/25/5 fuse/raycast/mesh) after a
-    warm-up of `warmup` requests. The budget is `budget_bytes`, or
+    warm-up that touches every session and `warmup` more requests. The
+    budget is `budget_bytes`, or
     `budget_frac` of all sessions' bytes, capped at 85 % of the free device
     memory. `pool_scale` multiplies every pool. Returns (list of per-rate
     summaries, executor)."""
@@ -457,6 +458,15 @@ def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, 
     try:
         sched = Scheduler(sizes, budget, max_mesh_per_tick=max_mesh_per_tick)
         if warmup:
+            # every session twice in order (restore, frame upload, render, result
+            # buffers; under a tight budget the second pass evicts every session
+            # once, allocating its snapshot buffer), meshes of the 16 largest
+            # pools (mesh buffers at full size), then `warmup` requests at the
+            # highest rate: first-touch costs stay out of the runs
+            for _ in range(2):
+                serve([Request(k, s, 0.0, 0) for s in range(n_sessions) for k in ("fuse", "raycast")], sched, ex)
+            big = sorted(range(n_sessions), key=lambda s: -wls[s].num_blocks)[:16]
+            serve([Request("mesh", s, 0.0, 0) for s in big], sched, ex)
             serve(poisson_requests(n_sessions, max(rates), warmup, seed=seed + 7), sched, ex)
         for k, rate in enumerate(rates):
             sched.evictions = sched.restores = 0
