@@ -164,6 +164,28 @@ vmap_status vmap_render_phong(const float* vmap_dev, size_t vmap_pitch, const fl
                               size_t nmap_pitch, uint8_t* rgba_dev, size_t rgba_pitch, int width, int height,
                               void* stream);
 
+/* ---- pipelined host frames (no counterpart in the reference, whose host
+ * path copies, computes and copies back one frame at a time). Enqueues one
+ * frame: its depth (and colour) are copied from host memory to one of two
+ * staging sets on an internal copy stream, fused and, when vmap_host is not
+ * NULL, rendered on `stream`, and the vertex (and normal) maps copied to host
+ * memory on a second internal copy stream. Returns at once; consecutive frames
+ * overlap their copies with each other's kernels. The host buffers must stay
+ * untouched until vmap_host_wait(map, stream) and then a synchronisation of
+ * `stream`: after vmap_host_wait, work on `stream` follows every copy of the
+ * frames enqueued so far. Pinned host buffers make the copies asynchronous. */
+typedef struct vmap_host_frame {
+    const void* depth_host;  /* width x height, packed                        */
+    int depth_type;          /* vmap_depth_type                               */
+    float depth_scale;       /* uint16 -> metres                              */
+    const uint8_t* rgb_host; /* uint8x3 packed, or NULL                       */
+    double pose[16];         /* camera-to-world, row-major                    */
+    float* vmap_host;        /* float4 vertex map out, or NULL (fuse only)    */
+    float* nmap_host;        /* float4 normal map out, or NULL                */
+} vmap_host_frame;
+vmap_status vmap_frame_host_async(vmap_map* map, const vmap_host_frame* frame, void* stream);
+vmap_status vmap_host_wait(vmap_map* map, void* stream);
+
 /* ---- meshing ------------------------------------------------------------- */
 /* Polygonize (marching_cubes.cu:251-305): marching cubes over all allocated
  * blocks. Writes at most max_tris triangles (9 floats each for verts and

@@ -53,6 +53,13 @@ class Stats(C.Structure):
         return {k: getattr(self, k) for k, _ in self._fields_}
 
 
+class HostFrame(C.Structure):
+    """vmap_host_frame: one frame for vmap_frame_host_async."""
+    _fields_ = [("depth_host", C.c_void_p), ("depth_type", C.c_int), ("depth_scale", C.c_float),
+                ("rgb_host", C.c_void_p), ("pose", C.c_double * 16), ("vmap_host", C.c_void_p),
+                ("nmap_host", C.c_void_p)]
+
+
 class LaunchConfig(C.Structure):
     """vmap_launch_config: grid of every stage in CTAs per SM (0 = default)."""
     _fields_ = [("alloc_ctas_per_sm", C.c_int), ("visibility_ctas_per_sm", C.c_int), ("fuse_ctas_per_sm", C.c_int),
@@ -101,6 +108,8 @@ SIGNATURES = {
     "vmap_create_in": (C.c_int, [C.POINTER(Config), P, C.c_uint64, P, C.POINTER(P)]),
     "vmap_batch_create_slots": (C.c_int, [C.c_int, C.c_int, C.POINTER(P)]),
     "vmap_batch_set_map": (C.c_int, [P, C.c_int, P]),
+    "vmap_frame_host_async": (C.c_int, [P, C.POINTER(HostFrame), P]),
+    "vmap_host_wait": (C.c_int, [P, P]),
     "vmap_get_launch_config": (C.c_int, [P, C.POINTER(LaunchConfig)]),
     "vmap_set_launch_config": (C.c_int, [P, C.POINTER(LaunchConfig)]),
     "vmap_batch_get_launch_config": (C.c_int, [P, C.POINTER(LaunchConfig)]),

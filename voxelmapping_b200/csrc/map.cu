@@ -37,6 +37,18 @@ struct vmap_map {
     float* hNorms;
     unsigned meshCap;
     unsigned* dNtri;
+    // pipelined host frames (vmap_frame_host_async): two staging sets, a copy
+    // stream each way, events ordering copies and kernels per set
+    struct HostPipe {
+        bool ready;
+        unsigned next;
+        cudaStream_t h2d, d2h;
+        void* depth[2];
+        uint8_t* rgb[2];
+        float4* vmap[2];
+        float4* nmap[2];
+        cudaEvent_t inReady[2], inFree[2], outReady[2], outFree[2];
+    } pipe;
     // stage timing: event pairs on the caller's stream
     unsigned tCap, tUsed;
     cudaEvent_t* tEv;
@@ -179,9 +191,28 @@ cudaError_t staged(vmap_map* m, int stage, cudaStream_t s, F&& launch)
     return e;
 }
 
+void pipe_free(vmap_map* m)
+{
+    vmap_map::HostPipe& p = m->pipe;
+    if (p.h2d) cudaStreamSynchronize(p.h2d);
+    if (p.d2h) cudaStreamSynchronize(p.d2h);
+    for (int b = 0; b < 2; ++b) {
+        cudaFree(p.depth[b]);
+        cudaFree(p.rgb[b]);
+        cudaFree(p.vmap[b]);
+        cudaFree(p.nmap[b]);
+        for (cudaEvent_t e : {p.inReady[b], p.inFree[b], p.outReady[b], p.outFree[b]})
+            if (e) cudaEventDestroy(e);
+    }
+    if (p.h2d) cudaStreamDestroy(p.h2d);
+    if (p.d2h) cudaStreamDestroy(p.d2h);
+    std::memset(&p, 0, sizeof(p));
+}
+
 void free_all(vmap_map* m)
 {
     timing_free(m);
+    pipe_free(m);
     if (!m->external) {  // buffers carved from caller memory stay with the caller
         cudaFree(m->dm.slots);
         cudaFree(m->dm.blockKeys);
@@ -607,6 +638,80 @@ vmap_status vmap_render_scene_host(vmap_map* m, const double pose[16], float* vm
     const size_t bytes = (size_t)m->cfg.width * m->cfg.height * sizeof(float4);
     VMAP_CK(cudaMemcpyAsync(vmap_host, m->dVmap, bytes, cudaMemcpyDeviceToHost, s));
     if (nmap_host) VMAP_CK(cudaMemcpyAsync(nmap_host, m->dNmap, bytes, cudaMemcpyDeviceToHost, s));
+    return VMAP_OK;
+}
+
+// Buffers, streams and events of the host pipeline, on its first use.
+static cudaError_t ensure_pipe(vmap_map* m)
+{
+    vmap_map::HostPipe& p = m->pipe;
+    if (p.ready) return cudaSuccess;
+    const size_t npix = (size_t)m->cfg.width * m->cfg.height;
+    cudaError_t e = cudaStreamCreateWithFlags(&p.h2d, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&p.d2h, cudaStreamNonBlocking);
+    for (int b = 0; b < 2 && e == cudaSuccess; ++b) {
+        e = cudaMalloc(&p.depth[b], npix * sizeof(float));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p.rgb[b], npix * 3);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p.vmap[b], npix * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&p.nmap[b], npix * sizeof(float4));
+        for (cudaEvent_t* ev : {&p.inReady[b], &p.inFree[b], &p.outReady[b], &p.outFree[b]})
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(ev, cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) {
+        pipe_free(m);
+        return e;
+    }
+    m->deviceBytes += 2 * npix * (sizeof(float) + 3 + 2 * sizeof(float4));
+    p.ready = true;
+    return cudaSuccess;
+}
+
+vmap_status vmap_frame_host_async(vmap_map* m, const vmap_host_frame* f, void* stream)
+{
+    if (!m || !f || !f->depth_host || !pose_ok(f->pose)) return VMAP_ERR_INVALID_ARG;
+    if (f->depth_type != VMAP_DEPTH_F32 && f->depth_type != VMAP_DEPTH_U16) return VMAP_ERR_INVALID_ARG;
+    if (f->depth_type == VMAP_DEPTH_U16 && !(f->depth_scale > 0)) return VMAP_ERR_INVALID_ARG;
+    if ((f->rgb_host && !m->cfg.with_color) || (f->nmap_host && !f->vmap_host)) return VMAP_ERR_INVALID_ARG;
+    VMAP_CK(ensure_pipe(m));
+    vmap_map::HostPipe& p = m->pipe;
+    cudaStream_t s = as_stream(stream);
+    const int b = (int)(p.next & 1u);
+    const size_t npix = (size_t)m->cfg.width * m->cfg.height;
+    const size_t elem = f->depth_type == VMAP_DEPTH_F32 ? 4 : 2;
+    // inputs: into staging set b once the fusion two frames back has read it
+    VMAP_CK(cudaStreamWaitEvent(p.h2d, p.inFree[b], 0));
+    VMAP_CK(cudaMemcpyAsync(p.depth[b], f->depth_host, npix * elem, cudaMemcpyHostToDevice, p.h2d));
+    if (f->rgb_host) VMAP_CK(cudaMemcpyAsync(p.rgb[b], f->rgb_host, npix * 3, cudaMemcpyHostToDevice, p.h2d));
+    VMAP_CK(cudaEventRecord(p.inReady[b], p.h2d));
+    // kernels on the caller's stream
+    VMAP_CK(cudaStreamWaitEvent(s, p.inReady[b], 0));
+    vmap_status st = fuse_impl(m, p.depth[b], f->depth_type, elem * m->cfg.width, f->depth_scale,
+                               f->rgb_host ? p.rgb[b] : nullptr, 3 * (size_t)m->cfg.width, f->pose, s);
+    if (st != VMAP_OK) return st;
+    VMAP_CK(cudaEventRecord(p.inFree[b], s));
+    if (f->vmap_host) {
+        // render into output set b once its copy-out two frames back is done
+        VMAP_CK(cudaStreamWaitEvent(s, p.outFree[b], 0));
+        st = vmap_render_scene(m, f->pose, (float*)p.vmap[b], 0, f->nmap_host ? (float*)p.nmap[b] : nullptr, 0,
+                               stream);
+        if (st != VMAP_OK) return st;
+        VMAP_CK(cudaEventRecord(p.outReady[b], s));
+        VMAP_CK(cudaStreamWaitEvent(p.d2h, p.outReady[b], 0));
+        VMAP_CK(cudaMemcpyAsync(f->vmap_host, p.vmap[b], npix * sizeof(float4), cudaMemcpyDeviceToHost, p.d2h));
+        if (f->nmap_host)
+            VMAP_CK(cudaMemcpyAsync(f->nmap_host, p.nmap[b], npix * sizeof(float4), cudaMemcpyDeviceToHost, p.d2h));
+        VMAP_CK(cudaEventRecord(p.outFree[b], p.d2h));
+    }
+    ++p.next;
+    return VMAP_OK;
+}
+
+vmap_status vmap_host_wait(vmap_map* m, void* stream)
+{
+    if (!m) return VMAP_ERR_INVALID_ARG;
+    if (!m->pipe.ready) return VMAP_OK;
+    cudaStream_t s = as_stream(stream);
+    for (int b = 0; b < 2; ++b) VMAP_CK(cudaStreamWaitEvent(s, m->pipe.outFree[b], 0));
     return VMAP_OK;
 }
 

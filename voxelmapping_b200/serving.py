@@ -458,12 +458,14 @@ def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, 
     try:
         sched = Scheduler(sizes, budget, max_mesh_per_tick=max_mesh_per_tick)
         if warmup:
-            # every session twice in order (restore, frame upload, render, result
-            # buffers; under a tight budget the second pass evicts every session
-            # once, allocating its snapshot buffer), meshes of the 16 largest
-            # pools (mesh buffers at full size), then `warmup` requests at the
-            # highest rate: first-touch costs stay out of the runs
-            for _ in range(2):
+            # every session once per distinct frame, in order (restores, frame
+            # uploads, renders, result buffers; every map fuses all its frames
+            # and reaches its steady size, and under a tight budget every
+            # session is evicted at that size, so its snapshot buffer is
+            # allocated), meshes of the 16 largest pools (mesh buffers at full
+            # size), then `warmup` requests at the highest rate: first-touch
+            # costs stay out of the measured runs
+            for _ in range(max(2, n_frames)):
                 serve([Request(k, s, 0.0, 0) for s in range(n_sessions) for k in ("fuse", "raycast")], sched, ex)
             big = sorted(range(n_sessions), key=lambda s: -wls[s].num_blocks)[:16]
             serve([Request("mesh", s, 0.0, 0) for s in big], sched, ex)
