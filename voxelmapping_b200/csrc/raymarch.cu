@@ -428,11 +428,14 @@ __global__ void __launch_bounds__(256, 4) raycast_kernel(const __grid_constant__
 template <class V, int FMT>
 static cudaError_t raycast_persistent(const V& views, const Launcher& l, cudaStream_t s)
 {
-    static int occ = 0;  // resident CTAs per SM of this instantiation
-    if (occ == 0) {
-        cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, raycast_kernel<V, FMT>, 256, 0);
-        if (e != cudaSuccess || occ < 1) occ = 1;
-    }
+    // resident CTAs per SM of this instantiation (a static initialiser runs
+    // once, thread-safely, on the first launch)
+    static const int occ = [] {
+        int o = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, raycast_kernel<V, FMT>, 256, 0) != cudaSuccess || o < 1)
+            o = 1;
+        return o;
+    }();
     // CTAs beyond those resident would only start once others finish: cap at occupancy
     const int per_sm = l.raycast > 0 && l.raycast < occ ? l.raycast : occ;
     raycast_kernel<V, FMT><<<stage_grid(l, per_sm), 256, 0, s>>>(views);
