@@ -522,13 +522,16 @@ def run_product(args):
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    traffic = None
+    traffic, l2_pct = None, None
     tf = ROOT / "profiles" / "ncu_traffic.json"
     if tf.exists():
-        traffic = json.loads(tf.read_text()).get(dom, {}).get("dram_bytes_per_launch")
+        entry = json.loads(tf.read_text()).get(dom, {})
+        traffic, l2_pct = entry.get("dram_bytes_per_launch"), entry.get("l2_throughput_pct")
     roof = {"kernel": dom, "bound": "hbm", "achieved": stages[dom]["gbs"], "peak": peak, "peak_source": peak_src,
             "unit": "GB/s", "frac": stages[dom]["gbs"] / peak, "traffic": traffic,
-            "alg_bytes_per_launch": stages[dom]["alg_bytes"]}
+            "alg_bytes_per_launch": stages[dom]["alg_bytes"],
+            # a latency-bound kernel: its L2 throughput (% of peak, one ncu capture) beside the HBM fraction
+            "l2_throughput_pct_ncu": l2_pct}
 
     line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_total_ms / args.steps,

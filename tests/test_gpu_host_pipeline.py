@@ -87,3 +87,19 @@ def test_pipeline_equals_synchronous_host_calls():
     assert lib.vmap_frame_host_async(b._map, C.byref(bad), None) == 1
     bad.depth_type, bad.nmap_host = L.DEPTH_U16, outs[0][1].data_ptr()  # normals without a vertex map
     assert lib.vmap_frame_host_async(b._map, C.byref(bad), None) == 1
+
+
+def test_python_host_pipeline_wrapper():
+    from voxelmapping_b200 import HostPipeline
+    sc = synth.Scene(WL)
+    frames = [sc.render(i) for i in range(0, 20, 5)]
+    a, b = new_map(), new_map()
+    pipe = HostPipeline(b)
+    outs = [pipe.submit(d, c, p) for d, c, p in frames]
+    pipe.wait()
+    for (d, c, p), (v, n) in zip(frames, outs):
+        a.FuseDepthAndImage(c, synth.depth_to_metres(d), p)
+        nm = torch.empty((WL.height, WL.width, 4), device="cuda")
+        va = a.RenderScene(None, p, nmap=nm).cpu().numpy()
+        assert np.array_equal(np.nan_to_num(va, nan=-9), np.nan_to_num(v, nan=-9))
+        assert np.array_equal(np.nan_to_num(nm.cpu().numpy(), nan=-9), np.nan_to_num(n, nan=-9))

@@ -265,6 +265,54 @@ class VoxelMapping:
         return {"coords": coords, "tsdf": tsdf, "weight": weight, "rgb": rgb}
 
 
+class HostPipeline:
+    """Frames from host memory through vmap_frame_host_async: copies of
+    neighbouring frames overlap each other's kernels.
+
+        pipe = HostPipeline(vm)
+        for depth, rgb, pose in frames:         # numpy arrays
+            vmap, nmap = pipe.submit(depth, rgb, pose)
+        pipe.wait()                              # every result is now in vmap / nmap
+
+    Inputs are copied into pinned buffers (so the caller may reuse its
+    arrays at once); each frame's results land in fresh pinned buffers,
+    returned as numpy arrays that hold them, complete after `wait()`."""
+
+    def __init__(self, vm, depth_scale=0.001, normals=True):
+        import torch
+        self.vm, self.scale, self.normals = vm, depth_scale, normals
+        self._torch = torch
+        self._keep = []
+
+    def submit(self, depth, rgb=None, pose=None, render=True):
+        torch = self._torch
+        vm = self.vm
+        d = torch.from_numpy(np.ascontiguousarray(depth)).pin_memory()
+        c = torch.from_numpy(np.ascontiguousarray(rgb)).pin_memory() if rgb is not None else None
+        f = L.HostFrame()
+        f.depth_host = d.data_ptr()
+        f.depth_type = L.DEPTH_F32 if d.dtype == torch.float32 else L.DEPTH_U16
+        f.depth_scale = self.scale
+        f.rgb_host = c.data_ptr() if c is not None else None
+        f.pose[:] = [float(x) for x in np.asarray(pose, np.float64).reshape(16)]
+        out = None
+        if render:
+            v = torch.empty((vm.height, vm.width, 4), dtype=torch.float32).pin_memory()
+            n = torch.empty_like(v).pin_memory() if self.normals else None
+            f.vmap_host = v.data_ptr()
+            f.nmap_host = n.data_ptr() if n is not None else None
+            out = (v.numpy(), n.numpy() if n is not None else None)
+        self._keep.append((d, c, out))
+        L.check(vm._lib.vmap_frame_host_async(vm._need(), C.byref(f), _stream()), "vmap_frame_host_async")
+        return out
+
+    def wait(self):
+        """Orders the current stream after every copy so far and synchronises it."""
+        L.check(self.vm._lib.vmap_host_wait(self.vm._need(), _stream()), "vmap_host_wait")
+        self._torch.cuda.current_stream().synchronize()
+        self._keep = []  # the returned arrays keep their own buffers alive
+
+
 class MapBatch:
     """Fuse + raycast many VoxelMapping maps per step (vmap_batch_*).
 
