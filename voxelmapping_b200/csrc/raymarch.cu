@@ -9,7 +9,8 @@
 // change the result is skipped:
 //   * inside an unallocated block, where the reference reads "invalid, 1.0"
 //     and steps one voxel at a time, the steps up to the block's exit are
-//     taken as one integer jump;
+//     taken as one integer jump; before the tile's nearest allocated block
+//     these jumps need no lookup and are taken when the ray starts;
 //   * when the 8 trilinear corners sit in the current block, the 7 besides
 //     the centre sample are read with independent loads (no lookups between);
 //   * hash lookups are cached per ray (current block + one neighbour).
@@ -167,6 +168,21 @@ struct March {
         return lerp8(s, c.ax, c.ay, c.az);
     }
 
+    // Every 1-voxel step inside the unallocated block (bx, by, bz) reads
+    // (1.0, invalid): jump to the first step past the block's exit (at least
+    // one step). Exit faces: +8 where the ray runs up (and +0), +0 where it
+    // runs down (and -0), so a zero component gives an infinite distance.
+    static __device__ __forceinline__ void empty_jump(Ray& r, int bx, int by, int bz)
+    {
+        const float tx = ((float)(bx * 8 + (signbit(r.dir.x) ? 0 : 8)) - r.res.x) * r.inv.x;
+        const float ty = ((float)(by * 8 + (signbit(r.dir.y) ? 0 : 8)) - r.res.y) * r.inv.y;
+        const float tz = ((float)(bz * 8 + (signbit(r.dir.z) ? 0 : 8)) - r.res.z) * r.inv.z;
+        const float t = fminf(fminf(tx, ty), tz);  // fminf drops the NaN of 0 * inf
+        const float k = fmaxf(1.f, ceilf(t - 1e-3f));
+        r.res = fma3(k, r.dir, r.res);
+        r.dist_s = __fadd_rn(r.dist_s, k);
+    }
+
     // Start a ray at pixel (x, y); false when it finishes at once (tile with
     // no allocated block: written as a miss).
     static __device__ __forceinline__ bool init(const MapView& v, Ray& r, int mi, int x, int y)
@@ -210,6 +226,17 @@ struct March {
                 r.dist_s = dist0 + k0;
             }
             r.dist_lim = fminf(dist_e, g * zf + 2.f);
+            // A sample nearer than zn (the nearest depth of any allocated block
+            // whose projection covers this tile, less a voxel) cannot lie in an
+            // allocated block: the loop would look its block up, find it empty
+            // and jump. Those jumps are taken here without lookups, with the
+            // loop's jump arithmetic: the same blocks and sample lattice (an
+            // instrumented run found every skipped block empty; positions agree
+            // with the lookup path to float rounding).
+            const float lim = g * zn - 1.f;
+            while (r.dist_s < lim && r.dist_s < r.dist_lim)
+                empty_jump(r, vox2blk(__float2int_rz(floorf(r.res.x))), vox2blk(__float2int_rz(floorf(r.res.y))),
+                           vox2blk(__float2int_rz(floorf(r.res.z))));
         }
         r.mi = mi;
         r.x = x;
@@ -249,17 +276,7 @@ struct March {
         const DevMap& m = v.m;
         const int bx = r.cbx, by = r.cby, bz = r.cbz;
         if (r.cblk < 0) {
-            // every 1-voxel step inside this unallocated block reads (1.0, invalid):
-            // jump to the last step still inside (at least one step). Exit faces:
-            // +8 where the ray runs up (and +0), +0 where it runs down (and -0),
-            // so a zero component gives an infinite distance.
-            const float tx = ((float)(bx * 8 + (signbit(r.dir.x) ? 0 : 8)) - r.res.x) * r.inv.x;
-            const float ty = ((float)(by * 8 + (signbit(r.dir.y) ? 0 : 8)) - r.res.y) * r.inv.y;
-            const float tz = ((float)(bz * 8 + (signbit(r.dir.z) ? 0 : 8)) - r.res.z) * r.inv.z;
-            const float t = fminf(fminf(tx, ty), tz);  // fminf drops the NaN of 0 * inf
-            const float k = fmaxf(1.f, ceilf(t - 1e-3f));
-            r.res = fma3(k, r.dir, r.res);
-            r.dist_s = __fadd_rn(r.dist_s, k);
+            empty_jump(r, bx, by, bz);
             r.sdf = 1.f;
             r.valid = false;
             return false;
