@@ -119,3 +119,123 @@ def test_poisson_mix_and_rate():
     gaps = np.diff([r.arrival for r in reqs])
     assert abs(gaps.mean() - 1e-3) < 5e-5 and gaps.min() >= 0
     assert len({r.session for r in reqs}) == 256
+
+
+class FakeAsyncMeshExecutor(FakeExecutor):
+    """Meshes finish 2.5e-4 s (simulated) after they start, like a mesh worker beside the ticks."""
+
+    def __init__(self, sched):
+        super().__init__(sched)
+        self.running = {}  # session -> (request, completion time)
+
+    def inflight(self):
+        for s in [s for s, (_, t) in self.running.items() if t <= self.t]:
+            r, t = self.running.pop(s)
+            r.done = t
+            self.log.append(r)
+        return frozenset(self.running)
+
+    def run_tick(self, plan, clock):
+        running = self.inflight()
+        touched = [s for s, _, _ in plan.batch] + [r.session for r in plan.mesh]
+        assert not set(touched) & running, "a session with a mesh in flight got new work"
+        assert not set(plan.evict) & running, "a session with a mesh in flight was evicted"
+        assert len(running) + len(plan.mesh) <= self.sched.max_mesh
+        mesh, plan.mesh = plan.mesh, []
+        super().run_tick(plan, clock)
+        for r in mesh:
+            self.running[r.session] = (r, self.t + 2.5e-4)
+
+
+@pytest.mark.parametrize("budget_frac", [1.0, 0.2])
+def test_meshes_in_flight_block_their_sessions(budget_frac):
+    rng = np.random.default_rng(4)
+    sizes = [int(x) for x in rng.integers(1, 20, 30) * 1000]
+    sched = S.Scheduler(sizes, max(max(sizes), int(sum(sizes) * budget_frac)), max_mesh_per_tick=2)
+    ex = FakeAsyncMeshExecutor(sched)
+    reqs = S.poisson_requests(30, 1e9, 2000, mix=(0.5, 0.2, 0.3), seed=5)
+    out, stats = S.serve(reqs, sched, ex, clock=lambda: ex.t, wait_until=lambda t: setattr(ex, "t", max(ex.t, t)))
+    assert all(np.isfinite(r.done) for r in out) and len(ex.log) == 2000
+    by_session = {}
+    for r in sorted(out, key=lambda r: (r.done, r.index)):
+        by_session.setdefault(r.session, []).append(r.index)
+    for s, idx in by_session.items():
+        assert idx == sorted(idx), s
+
+
+class StuckMeshExecutor(FakeAsyncMeshExecutor):
+    """A mesh that never finishes (a stopped worker): serve() must raise, not spin."""
+
+    def inflight(self):
+        return frozenset(self.running)
+
+
+def test_serve_raises_instead_of_spinning_on_a_stuck_mesh():
+    sched = S.Scheduler([10, 10], 100)
+    ex = StuckMeshExecutor(sched)
+    reqs = [S.Request("mesh", 0, 0.0, 0), S.Request("fuse", 0, 0.0, 1), S.Request("fuse", 1, 0.0, 2)]
+    with pytest.raises(RuntimeError, match="no progress"):
+        S.serve(reqs, sched, ex, clock=lambda: ex.t, wait_until=lambda t: setattr(ex, "t", max(ex.t, t)), stall_s=1.0)
+
+
+def _bare_executor(set_device, mesh_fn):
+    """GpuExecutor's mesh-worker machinery without a GPU: fake torch shim, fake mesh."""
+    import collections
+    import contextlib
+    import queue
+    import threading
+    import types
+    ex = S.GpuExecutor.__new__(S.GpuExecutor)
+    ex.torch = types.SimpleNamespace(cuda=types.SimpleNamespace(set_device=set_device,
+                                                                stream=lambda s: contextlib.nullcontext()))
+    ex.dev_index, ex.mesh_stream, ex.mesh_sp = 0, None, None
+    ex._mesh_q, ex._inflight, ex._lock, ex._worker_error = queue.Queue(), set(), threading.Lock(), None
+    ex.phase = collections.Counter()
+    ex._mesh = mesh_fn
+    ex._worker = threading.Thread(target=ex._mesh_loop, daemon=True)
+    ex._worker.start()
+    return ex
+
+
+def _submit(ex, reqs, clock):
+    for r in reqs:
+        with ex._lock:
+            ex._inflight.add(r.session)
+        ex._mesh_q.put((r, clock))
+
+
+def test_mesh_worker_completes_fails_and_stops_cleanly():
+    import time as T
+    clock = T.perf_counter
+
+    def mesh(s, stream, sp):
+        if s == 3:
+            raise ValueError("mesh failed")
+        return 100 + s
+    ex = _bare_executor(lambda i: None, mesh)
+    reqs = [S.Request("mesh", s, 0.0, s) for s in range(5)]
+    _submit(ex, reqs, clock)
+    t0 = T.perf_counter()
+    while ex.inflight() and T.perf_counter() - t0 < 10:
+        T.sleep(0.001)
+    assert not ex.inflight()
+    assert [r.result for r in reqs if r.session != 3] == [100, 101, 102, 104]
+    assert isinstance(reqs[3].result, ValueError) and all(np.isfinite(r.done) for r in reqs)
+    ex._mesh_q.put(None)
+    ex._worker.join(5)
+    assert not ex._worker.is_alive()
+
+
+def test_mesh_worker_that_cannot_start_fails_its_requests():
+    import time as T
+
+    def bad_set_device(i):
+        raise ValueError("no such device")
+    ex = _bare_executor(bad_set_device, lambda s, st, sp: 0)
+    ex._worker.join(5)
+    assert not ex._worker.is_alive() and isinstance(ex._worker_error, ValueError)
+    # requests handed to a dead worker are never served: inflight() reports it instead of hiding it
+    reqs = [S.Request("mesh", 0, 0.0, 0)]
+    _submit(ex, reqs, T.perf_counter)
+    with pytest.raises(RuntimeError, match="mesh worker stopped"):
+        ex.inflight()

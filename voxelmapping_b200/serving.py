@@ -30,6 +30,8 @@ import collections
 import ctypes as C
 import dataclasses
 import math
+import queue
+import threading
 import time
 from dataclasses import dataclass, field
 
@@ -86,6 +88,8 @@ class Scheduler:
     budget the bytes all resident sessions may hold together."""
 
     def __init__(self, session_bytes, budget, max_mesh_per_tick=2, max_resident=MAX_RESIDENT):
+        """max_mesh_per_tick: meshes started per tick, or in flight at once
+        when a mesh worker runs them beside the ticks."""
         self.bytes = list(session_bytes)
         if max(self.bytes) > budget:
             raise ValueError("a session needs more device memory than the whole budget")
@@ -106,14 +110,19 @@ class Scheduler:
     def free(self):
         return self.budget - self.used
 
-    def plan(self):
-        """Take the next tick's work off the queues."""
+    def plan(self, blocked=()):
+        """Take the next tick's work off the queues. `blocked`: sessions with
+        work still in flight from earlier ticks (meshes on the mesh worker):
+        they get no new work and are not evicted; they count against the
+        mesh limit."""
         p = TickPlan()
         heads = sorted((q[0].arrival, s) for s, q in self.queues.items() if q)
-        busy = set()
+        busy = set(blocked)
         for _, s in heads:
             q = self.queues[s]
-            if q[0].kind == "mesh" and len(p.mesh) >= self.max_mesh:
+            if s in busy:
+                continue
+            if q[0].kind == "mesh" and len(p.mesh) + len(blocked) >= self.max_mesh:
                 continue
             if s not in self.resident and (s in p.evict or not self._admit(s, busy, p)):
                 continue
@@ -173,12 +182,13 @@ class GpuExecutor:
     shared buffers and copied to one pinned host buffer."""
 
     def __init__(self, workloads, frames, device="cuda", copy_results=True, keep_results=False,
-                 n_slots=MAX_RESIDENT):
+                 n_slots=MAX_RESIDENT, mesh_worker=True):
         import torch
         self.torch = torch
         self.wls = list(workloads)
         self.frames = frames
         self.dev = torch.device(device)
+        self.dev_index = self.dev.index if self.dev.index is not None else torch.cuda.current_device()
         self.stream = torch.cuda.Stream(device=self.dev)
         self.sp = C.c_void_p(self.stream.cuda_stream)
         self.copy_results = copy_results
@@ -206,6 +216,64 @@ class GpuExecutor:
         self.mesh_count = torch.zeros(1, dtype=torch.int32, device=self.dev)
         self.mesh_count_host = torch.zeros(1, dtype=torch.int32, pin_memory=True)
         self.phase = collections.Counter()  # seconds per phase
+        # meshes run on their own stream in a worker thread, beside the ticks
+        # (the scheduler keeps their sessions out of the ticks meanwhile)
+        self.mesh_stream = torch.cuda.Stream(device=self.dev)
+        self.mesh_sp = C.c_void_p(self.mesh_stream.cuda_stream)
+        self._inflight = set()
+        self._worker_error = None
+        self._lock = threading.Lock()
+        self._mesh_q = queue.Queue() if mesh_worker else None
+        self._worker = None
+        if mesh_worker:
+            self._worker = threading.Thread(target=self._mesh_loop, name="vmap-mesh", daemon=True)
+            self._worker.start()
+
+    def inflight(self):
+        """Sessions whose mesh is still running on the mesh worker."""
+        with self._lock:
+            running = frozenset(self._inflight)
+        if running and self._worker is not None and not self._worker.is_alive():
+            raise RuntimeError("the mesh worker stopped with meshes in flight") from self._worker_error
+        return running
+
+    def _mesh_loop(self):
+        torch = self.torch
+        item = None
+        try:
+            torch.cuda.set_device(self.dev_index)
+            while True:
+                item = self._mesh_q.get()
+                if item is None:
+                    return
+                r, clock = item
+                try:
+                    t0 = clock()
+                    with torch.cuda.stream(self.mesh_stream):
+                        r.result = self._mesh(r.session, self.mesh_stream, self.mesh_sp)
+                    r.done = clock()
+                    self.phase["mesh"] += r.done - t0
+                except BaseException as e:  # surfaced by serve() through the request
+                    r.result = e
+                    r.done = clock()
+                finally:
+                    with self._lock:
+                        self._inflight.discard(r.session)
+                item = None
+        except BaseException as e:  # the worker itself failed: fail what it holds and stop
+            self._worker_error = e
+            pending = [item] if item is not None else []
+            while True:
+                try:
+                    nxt = self._mesh_q.get_nowait()
+                except queue.Empty:
+                    break
+                if nxt is not None:
+                    pending.append(nxt)
+            for r, clock in pending:
+                r.result, r.done = e, clock()
+            with self._lock:
+                self._inflight.clear()
 
     # -- memory ----------------------------------------------------------------
     def _new_map(self, s):
@@ -262,15 +330,15 @@ class GpuExecutor:
         f.depth_dev = f.rgb_dev = f.vmap_dev = f.nmap_dev = None
 
     # -- one tick ----------------------------------------------------------------
-    def _mesh(self, s):
-        """Full mesh of session s to pinned host memory; returns the triangle count."""
+    def _mesh(self, s, stream, sp):
+        """Full mesh of session s to pinned host memory on `stream`; returns the triangle count."""
         torch = self.torch
         vm = self.maps[s]
         lib = self.lib
-        L.check(lib.vmap_polygonize(vm._map, None, None, 0, C.c_void_p(self.mesh_count.data_ptr()), self.sp),
+        L.check(lib.vmap_polygonize(vm._map, None, None, 0, C.c_void_p(self.mesh_count.data_ptr()), sp),
                 "vmap_polygonize")
         self.mesh_count_host.copy_(self.mesh_count, non_blocking=True)
-        self.stream.synchronize()
+        stream.synchronize()
         n = int(self.mesh_count_host.item())
         if n == 0:
             return 0
@@ -282,10 +350,10 @@ class GpuExecutor:
                               torch.empty((cap, 9), dtype=torch.float32, pin_memory=True))
         v, nr = self.mesh_dev
         L.check(lib.vmap_polygonize(vm._map, C.c_void_p(v.data_ptr()), C.c_void_p(nr.data_ptr()), v.shape[0],
-                                    None, self.sp), "vmap_polygonize")
+                                    None, sp), "vmap_polygonize")
         self.mesh_host[0][:n].copy_(v[:n], non_blocking=True)
         self.mesh_host[1][:n].copy_(nr[:n], non_blocking=True)
-        self.stream.synchronize()
+        stream.synchronize()
         return n
 
     def run_tick(self, plan, clock):
@@ -345,11 +413,20 @@ class GpuExecutor:
             t3 = clock()
             self.phase["batch"] += t3 - t2
             for r in plan.mesh:
-                r.result = self._mesh(r.session)
-                r.done = clock()
-            self.phase["mesh"] += clock() - t3
+                if self._mesh_q is not None:
+                    with self._lock:
+                        self._inflight.add(r.session)
+                    self._mesh_q.put((r, clock))
+                else:
+                    r.result = self._mesh(r.session, self.stream, self.sp)
+                    r.done = clock()
+                    self.phase["mesh"] += r.done - t3
 
     def release(self):
+        if self._worker is not None:
+            self._mesh_q.put(None)
+            self._worker.join()
+            self._worker = None
         self.torch.cuda.synchronize()
         for s in list(self.maps):
             L.check(self.lib.vmap_batch_set_map(self.batch, self.slot[s], None), "vmap_batch_set_map")
@@ -360,11 +437,12 @@ class GpuExecutor:
             self.batch = None
 
 
-def serve(requests, scheduler, executor, clock=None, wait_until=None):
+def serve(requests, scheduler, executor, clock=None, wait_until=None, stall_s=120.0):
     """Replays `requests` (sorted by arrival) against wall-clock time: a
     request becomes visible to the scheduler at its arrival time; ticks run
     back to back while work is waiting. `clock` / `wait_until` replace the
-    wall clock and the idle wait (for simulated time). Returns
+    wall clock and the idle wait (for simulated time). Raises when work is
+    waiting or in flight and nothing completes for `stall_s` seconds. Returns
     (requests, stats)."""
     start = time.perf_counter()
     clock = clock or (lambda: time.perf_counter() - start)
@@ -374,21 +452,36 @@ def serve(requests, scheduler, executor, clock=None, wait_until=None):
             wait = t - clock()
             if wait <= 0:
                 return
-            if wait > 2e-4:
-                time.sleep(wait - 1e-4)
+            # sleeping (or yielding) releases the GIL to the mesh worker
+            time.sleep(wait - 1e-4 if wait > 2e-4 else 0)
 
     wait_until = wait_until or sleep_until
+    inflight = getattr(executor, "inflight", lambda: frozenset())  # sessions with a mesh still running
     pending = collections.deque(sorted(requests, key=lambda r: r.arrival))
     ticks, batch_sizes, busy = 0, [], 0.0
-    while pending or scheduler.waiting:
+    last_progress, last_state = clock(), None
+    while pending or scheduler.waiting or inflight():
         now = clock()
+        state = (ticks, inflight(), scheduler.waiting, len(pending))
+        if state != last_state:
+            last_state, last_progress = state, now
+        elif (scheduler.waiting or state[1]) and now - last_progress > stall_s:
+            raise RuntimeError("serving made no progress for %.0f s (%d waiting, meshes in flight for sessions %s)"
+                               % (now - last_progress, scheduler.waiting, sorted(state[1])))
         while pending and pending[0].arrival <= now:
             scheduler.submit(pending.popleft())
         if not scheduler.waiting:
-            wait_until(pending[0].arrival)
+            if inflight():
+                wait_until(min(pending[0].arrival, now + 1e-4) if pending else now + 1e-4)
+            else:
+                wait_until(pending[0].arrival)
             continue
-        plan = scheduler.plan()
+        blocked = inflight()
+        plan = scheduler.plan(blocked)
         if not plan.batch and not plan.mesh:
+            if blocked:  # the waiting work belongs to sessions whose meshes are running
+                wait_until(now + 1e-4)
+                continue
             raise RuntimeError("no admissible work: the budget cannot hold any waiting session")
         t0 = clock()
         executor.run_tick(plan, clock)
@@ -398,6 +491,9 @@ def serve(requests, scheduler, executor, clock=None, wait_until=None):
         ticks += 1
         batch_sizes.append(len(plan.batch))
     makespan = clock()
+    for r in requests:
+        if isinstance(r.result, BaseException):
+            raise RuntimeError("request %d (%s) failed" % (r.index, r.kind)) from r.result
     stats = {"ticks": ticks, "mean_batch": float(np.mean(batch_sizes)) if batch_sizes else 0.0,
              "max_batch": int(max(batch_sizes)) if batch_sizes else 0, "busy_s": busy, "makespan_s": makespan,
              "evictions": scheduler.evictions, "restores": scheduler.restores}
