@@ -522,14 +522,21 @@ def run_product(args):
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    traffic, l2_pct = None, None
+    traffic, l2_pct, traffic_capture, scale = None, None, None, None
     tf = ROOT / "profiles" / "ncu_traffic.json"
     if tf.exists():
         entry = json.loads(tf.read_text()).get(dom, {})
-        traffic, l2_pct = entry.get("dram_bytes_per_launch"), entry.get("l2_throughput_pct")
+        traffic_capture, l2_pct = entry.get("dram_bytes_per_launch"), entry.get("l2_throughput_pct")
+        # the capture is a smaller frame: scale its DRAM bytes to this run's
+        # launches by the units the kernel processes (visible blocks)
+        units = entry.get("visible_blocks_at_capture")
+        if traffic_capture is not None and units:
+            scale = float(vis.mean()) / units
+            traffic = traffic_capture * scale
     roof = {"kernel": dom, "bound": "hbm", "achieved": stages[dom]["gbs"], "peak": peak, "peak_source": peak_src,
             "unit": "GB/s", "frac": stages[dom]["gbs"] / peak, "traffic": traffic,
             "alg_bytes_per_launch": stages[dom]["alg_bytes"],
+            "traffic_at_capture": traffic_capture, "traffic_scale": scale,
             # a latency-bound kernel: its L2 throughput (% of peak, one ncu capture) beside the HBM fraction
             "l2_throughput_pct_ncu": l2_pct}
 
