@@ -372,6 +372,7 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
             "ratio_vs_plain": value / p_value, "megapixels_per_step": pixels / 1e6, "dtype": wls[0].voxel_format,
             "launch_config": launch_cfg, "tuning": tune_src,
             "hit_fraction_last_step": hits, "error_flags": int(np.bitwise_or.reduce([s["error_flags"] for s in stats])),
+            "maps_pool_full": int(sum(1 for s in stats if s["error_flags"] & L.FLAG_POOL_FULL)),
             "allocated_blocks_total": int(sum(s["allocated_blocks"] for s in stats))}
 
 
