@@ -118,7 +118,7 @@ def workload_config(wl, args, extra=None):
 class ClockSampler:
     FIELDS = ["index", "clocks.sm", "clocks.max.sm", "power.draw", "clocks_event_reasons.active",
               "clocks_event_reasons.hw_slowdown", "clocks_event_reasons.hw_thermal_slowdown",
-              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap"]
+              "clocks_event_reasons.sw_thermal_slowdown", "clocks_event_reasons.sw_power_cap", "utilization.gpu"]
 
     def __init__(self, gpu_id):
         self.gpu_id = gpu_id
@@ -127,7 +127,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             cmd = ["nvidia-smi", "--query-gpu=" + ",".join(self.FIELDS), "--format=csv,noheader,nounits", "-lms",
-                   "200"]
+                   "50"]
             if self.gpu_id is not None:
                 cmd += ["-i", str(self.gpu_id)]
             self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
@@ -145,15 +145,19 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        rows = [r.split(", ") for r in getattr(self, "out", "").strip().splitlines() if r.count(",") >= 8]
+        """Median SM clock and throttle reasons over the samples taken while
+        the GPU was busy (utilisation >= 50 %; all samples if none was)."""
+        rows = [r.split(", ") for r in getattr(self, "out", "").strip().splitlines() if r.count(",") >= 9]
         if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        num = lambda x: float(x) if x.strip().replace(".", "").isdigit() else None
+        busy = [r for r in rows if (num(r[9]) or 0.0) >= 50.0] or rows
+        sm = [num(r[1]) for r in busy if num(r[1]) is not None]
+        mx = [num(r[2]) for r in rows if num(r[2]) is not None]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
+        reasons = sorted({names[i] for r in busy for i in range(4) if r[5 + i].strip().lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "busy_samples": len(busy) if busy is not rows else 0}
 
 
 def gpu_index(local_rank):
@@ -472,14 +476,16 @@ def run_product(args):
     torch.cuda.synchronize()
     L.check(lib.vmap_timing_enable(h, args.steps * 8))
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    with ClockSampler(gpu_index(local)) as clk:
-        for k in range(args.steps):
-            flush.fill_(k & 255)
-            ev[k][0].record()
-            step(args.warmup + k)
-            ev[k][1].record()
-            L.check(lib.vmap_copy_counters(h, counters[k].data_ptr(), sp))
-        torch.cuda.synchronize()
+    # clocks are sampled from here through the e2e and batched arms' timed work
+    # (the plain loop alone lasts only tens of milliseconds)
+    clk = ClockSampler(gpu_index(local)).__enter__()
+    for k in range(args.steps):
+        flush.fill_(k & 255)
+        ev[k][0].record()
+        step(args.warmup + k)
+        ev[k][1].record()
+        L.check(lib.vmap_copy_counters(h, counters[k].data_ptr(), sp))
+    torch.cuda.synchronize()
     step_ms = [a.elapsed_time(b) for a, b in ev]
     stage_ms = (C.c_double * 7)()
     stage_n = (C.c_uint32 * 7)()
@@ -546,7 +552,7 @@ def run_product(args):
             "p50_ms": percentile(step_ms, 50), "p99_ms": percentile(step_ms, 99), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": wl.voxel_format, "data": "synthetic",
             "config": workload_config(wl, args), "roofline": roof, "stages": stages,
-            "gpu_launches": int(sum(stage_n)), "clocks": clk.summary(),
+            "gpu_launches": int(sum(stage_n)),
             "launch_config": launch_cfg, "tuning": tune_src,
             "map": {"allocated_blocks": int(st["allocated_blocks"]), "visible_blocks_mean": float(vis.mean()),
                     "error_flags": int(st["error_flags"])}}
@@ -665,6 +671,10 @@ def run_product(args):
         wls, desc = batched_uneven(args, rank)
         line["batched_uneven"] = run_batched(args, wls, dev, flush, world, distinct_frames=8)
         line["batched_uneven"]["config"] = desc
+
+    clk.__exit__(None, None, None)
+    line["clocks"] = clk.summary()
+    line["clocks"]["window"] = "plain, e2e and batched timed work"
 
     # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -273,3 +273,45 @@ def test_slot_batch_with_maps_in_caller_memory():
     L.check(lib.vmap_batch_destroy(h))
     for vm in slot_maps:
         vm.release()
+
+
+def test_set_map_on_a_regular_batch_records_again_and_matches_single_calls():
+    """vmap_batch_set_map on a batch made by vmap_batch_create (grids sized for
+    its original maps): after swapping a map in, steps still equal single-map
+    calls."""
+    import ctypes as C
+    wls = workloads()[:2]
+    scenes = [synth.Scene(wl) for wl in wls]
+    a, b = make_map(wls[0]), make_map(wls[1])
+    c = make_map(wls[1])  # replaces b after two steps
+    solo = [make_map(wls[0]), make_map(wls[1]), make_map(wls[1])]
+    batch = MapBatch([a, b])
+    side = torch.cuda.Stream()
+    for step in range(5):
+        cur = [a, b] if step < 2 else [a, c]
+        if step == 2:
+            L.check(L.lib().vmap_batch_set_map(batch._h, 1, c._map))
+            batch.maps[1] = c
+        fr = [sc.render(step * 4) for sc in scenes]
+        depths = [torch.from_numpy(d.view(np.int16)).cuda() for d, _, _ in fr]
+        rgbs = [torch.from_numpy(cc).cuda().reshape(wl.height, -1) if wl.with_color else None
+                for (_, cc, _), wl in zip(fr, wls)]
+        poses = [p for _, _, p in fr]
+        vb = [torch.empty((wl.height, wl.width, 4), device="cuda") for wl in wls]
+        torch.cuda.synchronize()
+        with torch.cuda.stream(side):
+            batch.step(depths, rgbs, poses, vb)
+        side.synchronize()
+        refs = [solo[0], solo[1] if step < 2 else solo[2]]
+        for i, (wl, vm) in enumerate(zip(wls, refs)):
+            if wl.with_color:
+                vm.FuseDepthAndImage(rgbs[i], depths[i], poses[i])
+            else:
+                vm.FuseDepth(depths[i], poses[i])
+            v = vm.RenderScene(None, poses[i])
+            torch.cuda.synchronize()
+            assert np.array_equal(np.nan_to_num(v.cpu().numpy(), nan=-9.0), np.nan_to_num(vb[i].cpu().numpy(), nan=-9.0)), (step, i)
+    assert c.stats()["allocated_blocks"] == solo[2].stats()["allocated_blocks"] > 0
+    # the same map in two slots is refused
+    assert L.lib().vmap_batch_set_map(batch._h, 0, c._map) == 1
+    batch.release()
