@@ -253,8 +253,9 @@ vmap_status vmap_batch_step(vmap_batch* batch, const vmap_batch_frame* frames, v
  * items, so any shape gives the same results and only the time changes.
  * 0 in a field selects the library default (alloc 8, visibility 2, fuse 16,
  * zrange 4, normals 8, mesh 8; raycast 0 = as many CTAs as fit on an SM, the
- * ray marcher being persistent). Values above 64 are refused. Setting a
- * batch's shapes synchronises the device and records its graphs again. */
+ * ray marcher being persistent). Values above 64 (tile orders above 2) are
+ * refused. Setting a batch's shapes synchronises the device and records its
+ * graphs again. */
 typedef struct vmap_launch_config {
     int alloc_ctas_per_sm;
     int visibility_ctas_per_sm;
@@ -263,6 +264,11 @@ typedef struct vmap_launch_config {
     int raycast_ctas_per_sm;
     int normals_ctas_per_sm;
     int mesh_ctas_per_sm;
+    /* order in which the ray marcher hands out each image's pixel tiles:
+     * 0 = default (bottom rows first), 1 = top rows first, 2 = alternating
+     * from both ends. Tiles are independent, so only the time changes: the
+     * slowest tiles are best started first. */
+    int raycast_tile_order;
 } vmap_launch_config;
 vmap_status vmap_get_launch_config(const vmap_map* map, vmap_launch_config* out);
 vmap_status vmap_set_launch_config(vmap_map* map, const vmap_launch_config* cfg);

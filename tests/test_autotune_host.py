@@ -29,4 +29,5 @@ def test_store_and_lookup(tmp_path, monkeypatch):
 def test_candidates_are_valid_launch_values():
     for f in AT.FIELDS:
         assert all(0 <= c <= 64 for c in AT.CANDIDATES[f]), f
-    assert set(AT.STAGE) | {"mesh_ctas_per_sm"} == set(AT.FIELDS)
+    assert set(AT.CANDIDATES["raycast_tile_order"]) == {0, 1, 2}
+    assert set(AT.STAGE) | {"mesh_ctas_per_sm", "raycast_tile_order"} == set(AT.FIELDS)

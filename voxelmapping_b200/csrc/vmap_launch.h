@@ -24,6 +24,7 @@ struct Launcher {
     int alloc = 8, visibility = 2, fuse = 16, zrange = 4;
     int raycast = 0;  // persistent ray marcher: 0 = as many CTAs as fit on an SM
     int normals = 8, mesh = 8;
+    int tileOrder = 0;  // ray-marcher tile order (vmap_launch_config.raycast_tile_order)
 };
 
 // vmap_launch_config <-> Launcher (0 in a field: the default)
@@ -33,7 +34,7 @@ inline bool launch_config_ok(const vmap_launch_config* c)
                       c->raycast_ctas_per_sm, c->normals_ctas_per_sm, c->mesh_ctas_per_sm};
     for (int x : v)
         if (x < 0 || x > 64) return false;
-    return true;
+    return c->raycast_tile_order >= 0 && c->raycast_tile_order <= 2;
 }
 
 inline void launch_config_to(const vmap_launch_config* c, Launcher& l)
@@ -46,6 +47,7 @@ inline void launch_config_to(const vmap_launch_config* c, Launcher& l)
     l.raycast = c->raycast_ctas_per_sm;
     l.normals = c->normals_ctas_per_sm ? c->normals_ctas_per_sm : d.normals;
     l.mesh = c->mesh_ctas_per_sm ? c->mesh_ctas_per_sm : d.mesh;
+    l.tileOrder = c->raycast_tile_order;
 }
 
 inline void launch_config_from(const Launcher& l, vmap_launch_config* c)
@@ -57,6 +59,7 @@ inline void launch_config_from(const Launcher& l, vmap_launch_config* c)
     c->raycast_ctas_per_sm = l.raycast;
     c->normals_ctas_per_sm = l.normals;
     c->mesh_ctas_per_sm = l.mesh;
+    c->raycast_tile_order = l.tileOrder;
 }
 
 // grid of `per_sm` CTAs per SM, or fewer when there are fewer work items
