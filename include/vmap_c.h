@@ -14,9 +14,11 @@
  *  - Device pointers (`_dev`) must be CUDA device memory; `_host` pointers host
  *    memory (pinned for asynchronous copies). Pitches are in bytes.
  *  - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
- *    All calls are asynchronous on that stream unless documented otherwise;
- *    no call synchronises the device or reads counters back to the host
- *    except vmap_get_stats / vmap_polygonize_host / the *_host variants.
+ *    All calls are asynchronous on that stream unless documented otherwise.
+ *    The fuse / render / mesh / batch-step path never synchronises; the calls
+ *    that do are marked at their declaration: vmap_create / vmap_destroy,
+ *    vmap_get_stats, vmap_polygonize_host, the host-buffer variants, the block
+ *    exports, the snapshot calls and the batch reconfiguration calls.
  *  - Errors: every call returns a vmap_status. Conditions detected on the GPU
  *    (pool or hash table full, coordinates out of range, mesh buffer full) are
  *    accumulated as sticky flags read by vmap_get_stats. Nothing calls exit().
