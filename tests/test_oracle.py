@@ -1,0 +1,108 @@
+"""Known-answer tests of the CPU oracle (no GPU): a fronto-parallel wall at a
+known depth has a closed-form TSDF and surface, so fusion, ray marching and
+marching cubes can be checked against geometry, in both the FP32
+reference-arithmetic mode and the FP64 mode; plus the reference's validity
+rules (depth range, NaN), weight cap and colour blend (depth_fusion.cu:148-196,
+328-380; map_struct.h:9-10)."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+W, H, F = 64, 48, 50.0
+K = np.array([[F, 0, (W - 1) / 2], [0, F, (H - 1) / 2], [0, 0, 1]])
+VS = 0.008
+MU = np.float32(VS) * np.float32(4)
+D = 1.0
+POSE = np.eye(4)
+
+
+def wall(depth=D):
+    return np.full((H, W), depth, np.float32)
+
+
+@pytest.mark.parametrize("precision", [O.FP32, O.FP64])
+def test_wall_tsdf_matches_projective_distance(precision):
+    om = O.OracleMap(W, H, K, 4096, VS, precision=precision, storage="f32", with_color=False)
+    res = om.fuse(wall(), None, POSE)
+    assert res["visible"] > 0 and res["failed"] == 0
+    e = om.export()
+    assert len(e["coords"]) > 0
+    # voxel corner points (block * 8 + local) * vs, local index x + 8y + 64z
+    loc = np.arange(512)
+    lx, ly, lz = loc % 8, (loc // 8) % 8, loc // 64
+    z = (e["coords"][:, 2:3] * 8 + lz[None, :]) * VS
+    w = e["weight"]
+    assert set(np.unique(w)) <= {0.0, 1.0}
+    obs = w > 0
+    want = np.minimum(1.0, (D - z) / MU)
+    assert np.abs(e["tsdf"][obs] - want[obs]).max() < 1e-5
+    # observed exactly where the voxel projects into the image and lies at most mu behind the wall
+    assert (z[obs] <= D + MU + 1e-6).all()
+    assert np.isclose(w[(np.abs(z - D) < 0.5 * float(MU))].mean(), 1.0, atol=0.2)
+
+
+@pytest.mark.parametrize("precision", [O.FP32, O.FP64])
+def test_wall_raycast_and_mesh_lie_on_the_wall(precision):
+    om = O.OracleMap(W, H, K, 4096, VS, precision=precision, storage="f32", with_color=False)
+    for _ in range(2):
+        om.fuse(wall(), None, POSE)
+    v = om.raycast(POSE)
+    hit = np.isfinite(v[..., 0])
+    assert hit[4:-4, 4:-4].mean() > 0.95
+    assert np.abs(v[hit][:, 2] - D).max() < 1e-3  # a linear field: trilinear + refinement land on it
+    assert (v[hit][:, 3] == 1.0).all()
+    n, verts, norms = om.polygonize()
+    assert n > 100
+    zs = verts.reshape(-1, 3)[:, 2]
+    assert np.abs(zs - D).max() < 1e-4
+    nz = norms.reshape(-1, 3)[:, 2]
+    assert (np.abs(np.abs(nz) - 1.0) < 1e-3).mean() > 0.95  # facing the camera
+
+
+def test_depth_validity_rules():
+    for depth in (0.0, 0.05, 5.5, np.nan):
+        om = O.OracleMap(W, H, K, 4096, VS, storage="f32", with_color=False)
+        res = om.fuse(wall(depth), None, POSE)
+        assert om.num_blocks() == 0 and res["visible"] == 0, depth
+    om = O.OracleMap(W, H, K, 4096, VS, storage="f32", with_color=False)
+    om.fuse(wall(4.9), None, POSE)
+    assert om.num_blocks() > 0
+
+
+def test_weight_cap_and_colour_blend():
+    om = O.OracleMap(W, H, K, 4096, VS, storage="f32", max_weight=3, with_color=True)
+    c1 = np.full((H, W, 3), (100, 40, 250), np.uint8)
+    c2 = np.full((H, W, 3), (200, 90, 10), np.uint8)
+    om.fuse(wall(), c1, POSE)
+    e1 = om.export()
+    obs1 = e1["weight"] > 0
+    assert (e1["rgb"][obs1] == (100, 40, 250)).all()  # first observation copies the colour
+    om.fuse(wall(), c2, POSE)
+    e2 = om.export()
+    obs2 = e2["weight"] > 0
+    want = np.floor(0.7 * np.array([100, 40, 250]) + 0.3 * np.array([200, 90, 10]) + 1e-4).astype(np.uint8)
+    seen_twice = e2["weight"] == 2
+    assert seen_twice.any() and (e2["rgb"][seen_twice] == want).all()
+    for _ in range(4):
+        om.fuse(wall(), c2, POSE)
+    assert om.export()["weight"].max() == 3
+
+
+def test_fp32_and_fp64_modes_agree_on_a_room_frame():
+    from voxelmapping_b200 import synth
+    wl = synth.WORKLOADS["room_small"]
+    d, _, pose = synth.Scene(wl).render(0, noisy=False, dropout=0.0)
+    dm = synth.depth_to_metres(d)
+    maps = [O.OracleMap(wl.width, wl.height, wl.K, 1 << 16, wl.voxel_size, precision=p, storage="f32")
+            for p in (O.FP32, O.FP64)]
+    for om in maps:
+        om.fuse(dm, None, pose)
+    k32, k64 = (set(map(tuple, om.export()["coords"])) for om in maps)
+    # a sample on a block boundary can round into either neighbour (0.4 % of
+    # blocks on this noise-free frame)
+    assert len(k32 ^ k64) <= 1e-2 * len(k32)
+    v32, v64 = (om.raycast(pose) for om in maps)
+    both = np.isfinite(v32[..., 0]) & np.isfinite(v64[..., 0])
+    assert both.mean() > 0.5
+    assert (np.abs(v32[..., 2][both] - v64[..., 2][both]) <= 1e-3).mean() > 0.999
