@@ -106,3 +106,45 @@ def test_fp32_and_fp64_modes_agree_on_a_room_frame():
     both = np.isfinite(v32[..., 0]) & np.isfinite(v64[..., 0])
     assert both.mean() > 0.5
     assert (np.abs(v32[..., 2][both] - v64[..., 2][both]) <= 1e-3).mean() >= 0.995
+
+
+def sphere_depth(center, radius):
+    """Depth image of a sphere seen from the origin along +z (NaN where missed)."""
+    u, v = np.meshgrid(np.arange(W, dtype=np.float64), np.arange(H, dtype=np.float64))
+    d = np.stack([(u - K[0, 2]) / F, (v - K[1, 2]) / F, np.ones_like(u)], -1)  # ray with z = 1
+    c = np.asarray(center, np.float64)
+    a = (d * d).sum(-1)
+    b = (d * c).sum(-1)
+    disc = b * b - a * ((c * c).sum() - radius * radius)
+    t = (b - np.sqrt(np.maximum(disc, 0))) / a  # depth = t (z component of the ray is 1)
+    return np.where(disc > 0, t, np.nan).astype(np.float32)
+
+
+@pytest.mark.parametrize("precision", [O.FP32, O.FP64])
+def test_sphere_raycast_lands_on_the_surface(precision):
+    center, radius = (0.05, -0.03, 1.2), 0.35
+    depth = sphere_depth(center, radius)
+    om = O.OracleMap(W, H, K, 8192, VS, precision=precision, storage="f32", with_color=False)
+    om.fuse(np.nan_to_num(depth, nan=0.0), None, POSE)
+    v = om.raycast(POSE)
+    hit = np.isfinite(v[..., 0])
+    inside = np.isfinite(depth)
+    core = inside & (np.abs(depth - depth[inside].min()) < 0.15)  # away from the grazing rim
+    assert hit[core].mean() > 0.98
+    pts = v[hit & core][:, :3].astype(np.float64)
+    r = np.linalg.norm(pts - np.array(center), axis=-1)
+    assert np.abs(r - radius).max() < 2e-3  # within a quarter voxel of the analytic surface
+
+
+def test_normals_of_a_planar_vertex_map():
+    # vertices of the plane z = 1 + 0.5 x: the normal is (-0.5, 0, 1) normalised, up to sign
+    u, v = np.meshgrid(np.arange(W, dtype=np.float32), np.arange(H, dtype=np.float32))
+    x = (u - 31.5) / 50.0
+    y = (v - 23.5) / 50.0
+    z = 1.0 + 0.5 * x
+    vm = np.stack([x, y, z, np.ones_like(x)], -1).astype(np.float32)
+    nm = O.compute_normal(vm)
+    want = np.array([-0.5, 0.0, 1.0]) / np.linalg.norm([-0.5, 0.0, 1.0])
+    interior = nm[1:-1, 1:-1, :3].reshape(-1, 3)
+    assert np.abs(np.abs(interior @ want) - 1.0).max() < 1e-5
+    assert np.isnan(nm[-1]).all() and np.isnan(nm[:, -1]).all()  # last row and column are undefined
