@@ -178,26 +178,58 @@ def gpu_index(local_rank):
 
 
 # -------------------------------------------------------------- CPU baseline
-def cpu_oracle_run(wl, frames, n_threads, seconds=None, steps=None):
+def cpu_oracle_run(wl, frames, n_threads, seconds=None, steps=None, om=None):
     """Reference algorithm (FP32 restatement, same voxel format) on the host:
-    fuse + raycast per frame. Returns per-frame seconds."""
+    fuse, then raycast + normal map, per frame, like one GPU step. Returns the
+    oracle map and per-frame seconds of the two stages."""
     from oracle import oracle as O
     from voxelmapping_b200 import synth
     O.set_threads(n_threads)
-    om = O.OracleMap(wl.width, wl.height, wl.K, wl.num_blocks, wl.voxel_size, storage=wl.voxel_format,
-                     max_weight=wl.max_weight, with_color=wl.with_color)
-    times = []
+    if om is None:
+        om = O.OracleMap(wl.width, wl.height, wl.K, wl.num_blocks, wl.voxel_size, storage=wl.voxel_format,
+                         max_weight=wl.max_weight, with_color=wl.with_color)
+    st = {"fuse": [], "raycast": []}
     t_start = time.perf_counter()
-    for i, (d, rgb, pose) in enumerate(frames):
+    for d, rgb, pose in frames:
         t0 = time.perf_counter()
         om.fuse(synth.depth_to_metres(d, wl.depth_scale), rgb if wl.with_color else None, pose)
-        om.raycast(pose)
-        times.append(time.perf_counter() - t0)
+        t1 = time.perf_counter()
+        O.compute_normal(om.raycast(pose))
+        st["fuse"].append(t1 - t0)
+        st["raycast"].append(time.perf_counter() - t1)
         if seconds is not None and time.perf_counter() - t_start > seconds:
             break
-        if steps is not None and len(times) >= steps:
+        if steps is not None and len(st["fuse"]) >= steps:
             break
-    return times
+    return om, st
+
+
+def cpu_baseline(wl, scene, frames, threads, seconds=None, skip=0, one_thread_frames=2):
+    """The oracle on the host cores: frames/s over `frames` (after `skip`
+    untimed ones) with `threads` threads, per-stage p50 / p99, one mesh
+    extraction of the resulting map, and the next `one_thread_frames` frames
+    on one thread."""
+    from oracle import oracle as O
+    om, st = cpu_oracle_run(wl, frames, threads, seconds=seconds)
+    used = len(st["fuse"])
+    fr = [f + r for f, r in zip(st["fuse"], st["raycast"])][skip:]
+    ms = lambda xs: {"p50": 1e3 * percentile(xs, 50), "p99": 1e3 * percentile(xs, 99)}
+    out = {"value": len(fr) / sum(fr), "unit": "frames/s", "cores": threads, "kind": "port",
+           "frames_timed": len(fr), "frame_ms": ms(fr), "fuse_ms": ms(st["fuse"][skip:]),
+           "raycast_normals_ms": ms(st["raycast"][skip:])}
+    t0 = time.perf_counter()
+    n, _, _ = om.polygonize()
+    out["mesh"] = {"ms": 1e3 * (time.perf_counter() - t0), "triangles": int(n), "threads": threads,
+                   "map_frames": used}
+    if one_thread_frames > 0:
+        nxt = [frames[i] if i < len(frames) else scene.render(i) for i in range(used, used + one_thread_frames)]
+        _, st1 = cpu_oracle_run(wl, nxt, 1, om=om)
+        fr1 = [f + r for f, r in zip(st1["fuse"], st1["raycast"])]
+        out["one_thread"] = {"frames/s": len(fr1) / sum(fr1), "frame_ms": ms(fr1), "fuse_ms": ms(st1["fuse"]),
+                             "raycast_normals_ms": ms(st1["raycast"]),
+                             "sample": "frames %d..%d on the same map" % (used, used + len(fr1) - 1)}
+        O.set_threads(threads)
+    return out
 
 
 def run_reference(args):
@@ -209,19 +241,17 @@ def run_reference(args):
     scene = synth.Scene(wl)
     frames = [scene.render(i) for i in range(args.warmup + args.steps)]
     threads = os.cpu_count() or 1
-    times = cpu_oracle_run(wl, frames, threads)
-    timed = times[args.warmup:]
-    total = sum(timed)
-    value = len(timed) / total
+    cb = cpu_baseline(wl, scene, frames, threads, skip=args.warmup)
+    value = cb["value"]
+    cb["sample"] = ("frames %d..%d of %s, fuse + raycast + normals each (every step a full frame)"
+                    % (args.warmup, args.warmup + args.steps - 1, WORKLOAD))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(timed),
-            "p50_ms": 1e3 * percentile(timed, 50), "p99_ms": 1e3 * percentile(timed, 99),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value,
+            "p50_ms": cb["frame_ms"]["p50"], "p99_ms": cb["frame_ms"]["p99"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": wl.voxel_format,
             "data": "synthetic",
             "config": workload_config(wl, args, {"path": "reference algorithm, CPU restatement (oracle port)"}),
-            "cpu_baseline": {"value": value, "unit": "frames/s", "cores": threads, "kind": "port",
-                             "sample": "frames %d..%d of %s, fuse + raycast each (every step a full frame)"
-                                       % (args.warmup, args.warmup + args.steps - 1, WORKLOAD)},
+            "cpu_baseline": cb,
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -679,11 +709,10 @@ def run_product(args):
     # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        times = cpu_oracle_run(wl, frames, threads, seconds=args.cpu_seconds)
-        line["cpu_baseline"] = {"value": len(times) / sum(times), "unit": "frames/s", "cores": threads,
-                                "kind": "port",
-                                "sample": "frames 0..%d of %s (fuse + raycast each, FP32 reference-algorithm "
-                                          "restatement, %d threads)" % (len(times) - 1, WORKLOAD, threads)}
+        cb = cpu_baseline(wl, scene, frames, threads, seconds=args.cpu_seconds)
+        cb["sample"] = ("frames 0..%d of %s (fuse + raycast + normals each, FP32 reference-algorithm "
+                        "restatement, %d threads)" % (cb["frames_timed"] - 1, WORKLOAD, threads))
+        line["cpu_baseline"] = cb
     if args.serving:
         from voxelmapping_b200 import serving as S
         rates = [float(r) for r in args.serving_rates.split(",")]

@@ -1,0 +1,31 @@
+"""`bench.py --impl reference` on CPU: the oracle port on the host cores prints
+one JSON line with the bench contract's keys, the per-stage CPU times (fuse,
+raycast + normals, mesh) and a one-thread sample."""
+import json
+import os
+import subprocess
+import sys
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+def test_reference_arm_prints_one_contract_line():
+    env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "2", "--warmup", "1"],
+                         cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [l for l in out.stdout.splitlines() if l.strip()]
+    assert len(lines) == 1
+    line = json.loads(lines[0])
+    assert line["impl"] == "reference" and line["unit"] == "frames/s" and line["higher_is_better"] is True
+    assert line["steps"] == 2 and line["warmup"] == 1 and line["value"] > 0
+    cb = line["cpu_baseline"]
+    assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"]
+    assert cb["frames_timed"] == 2 and "frames 1..2" in cb["sample"]
+    for k in ("frame_ms", "fuse_ms", "raycast_normals_ms"):
+        assert 0 < cb[k]["p50"] <= cb[k]["p99"]
+    assert cb["mesh"]["triangles"] > 0 and cb["mesh"]["ms"] > 0
+    assert cb["one_thread"]["frames/s"] > 0
+    assert line["e2e"] == {"value": line["value"], "unit": "frames/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
