@@ -29,3 +29,16 @@ def test_reference_arm_prints_one_contract_line():
     assert cb["one_thread"]["frames/s"] > 0
     assert line["e2e"] == {"value": line["value"], "unit": "frames/s", "h2d_bytes_per_step": 0,
                            "d2h_bytes_per_step": 0}
+
+
+def test_cpu_baseline_renders_frames_past_the_sample_for_the_one_thread_run():
+    sys.path.insert(0, str(ROOT))
+    import bench
+    from voxelmapping_b200 import synth
+    wl = synth.WORKLOADS["room_small"]
+    scene = synth.Scene(wl)
+    frames = [scene.render(i) for i in range(2)]
+    cb = bench.cpu_baseline(wl, scene, frames, 2, seconds=30.0)
+    assert cb["frames_timed"] == 2 and cb["cores"] == 2
+    assert cb["one_thread"]["sample"] == "frames 2..3 on the same map"
+    assert cb["mesh"]["map_frames"] == 2 and cb["mesh"]["triangles"] > 0
