@@ -340,9 +340,9 @@ vmap_status vmap_snapshot_load(vmap_map* map, const void* src, uint64_t bytes, v
  * Same output as vmap_export_blocks for the blocks [first, first + count) in
  * pool order: count <= VMAP_EXPORT_STATIC_MAX_BLOCKS; *n_blocks receives how
  * many exist from `first` on. It is for callers that must not call cudaMalloc
- * or cudaFree once running: loops under a no-allocation policy, plugins whose
- * host owns all device memory, code running while a stream is captured into a
- * CUDA graph. vmap_export_blocks stages through device buffers it allocates on
+ * or cudaFree once running: loops under a no-allocation policy (an allocation
+ * can stall or fail mid-run), plugins whose host owns all device memory.
+ * vmap_export_blocks stages through device buffers it allocates on
  * every call; this entry point stages through one fixed device array of
  * VMAP_EXPORT_STATIC_MAX_BLOCKS blocks (about 1.4 MiB) that every GPU loading
  * the library holds until the process exits.

@@ -1,8 +1,8 @@
 """vmap_export_blocks_static: the block export for callers that cannot allocate.
 
-Callers running under a no-allocation policy, inside a host application that
-owns all device memory, or while a stream is being captured into a CUDA graph
-cannot use vmap_export_blocks, which allocates device staging on every call.
+Callers running under a no-allocation policy, or inside a host application
+that owns all device memory, cannot use vmap_export_blocks, which allocates
+device staging on every call.
 The static variant stages through a fixed device array instead. Here it must
 return exactly what vmap_export_blocks returns (the export is exact, so the
 tolerance is zero), on two calls in a row over the same map, and refuse

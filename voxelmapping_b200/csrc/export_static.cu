@@ -2,10 +2,9 @@
 //
 // vmap_export_blocks stages each chunk of blocks in device buffers it
 // cudaMalloc's and frees on every call. Some callers must not allocate once
-// they are running: a real-time loop under a no-allocation policy, a plugin
-// whose host application owns all device memory, code that runs while a
-// stream is being captured into a CUDA graph (where cudaMalloc is not
-// allowed). This entry point stages through one fixed array in device
+// they are running: a real-time loop under a no-allocation policy (an
+// allocation can stall or fail mid-run), a plugin whose host application owns
+// all device memory. This entry point stages through one fixed array in device
 // global memory instead, sized for VMAP_EXPORT_STATIC_MAX_BLOCKS blocks, and
 // copies the result into the caller's host buffers.
 //
