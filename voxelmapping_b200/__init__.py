@@ -5,6 +5,6 @@ include/vmap_c.h; this package holds its ctypes binding, the Python mirror of
 the reference's VoxelMapping class and the synthetic-scene generator.
 """
 from ._lib import VmapError, lib  # noqa: F401
-from .vmapping import HostPipeline, MapBatch, VoxelMapping  # noqa: F401
+from .vmapping import HostPipeline, MapBatch, VoxelMapping, snapshot_header  # noqa: F401
 
-__all__ = ["VoxelMapping", "MapBatch", "HostPipeline", "VmapError", "lib"]
+__all__ = ["VoxelMapping", "MapBatch", "HostPipeline", "snapshot_header", "VmapError", "lib"]

@@ -67,6 +67,15 @@ class LaunchConfig(C.Structure):
                 ("mesh_ctas_per_sm", C.c_int), ("raycast_tile_order", C.c_int)]
 
 
+class SnapshotHeader(C.Structure):
+    """vmap_snapshot_header: the first 64 bytes of a vmap_snapshot_save image."""
+    _fields_ = [("magic", C.c_char * 8), ("version", C.c_uint32), ("header_bytes", C.c_uint32),
+                ("voxel_format", C.c_int32), ("with_color", C.c_int32), ("block_bytes", C.c_uint32),
+                ("n_blocks", C.c_uint32), ("voxel_size", C.c_float), ("truncation", C.c_float),
+                ("max_weight", C.c_int32), ("error_flags", C.c_uint32), ("keys_offset", C.c_uint64),
+                ("pool_offset", C.c_uint64)]
+
+
 class BatchFrame(C.Structure):
     _fields_ = [("depth_dev", C.c_void_p), ("depth_type", C.c_int), ("depth_pitch", C.c_size_t),
                 ("depth_scale", C.c_float), ("rgb_dev", C.c_void_p), ("rgb_pitch", C.c_size_t),

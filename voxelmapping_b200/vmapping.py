@@ -265,6 +265,27 @@ class VoxelMapping:
         return {"coords": coords, "tsdf": tsdf, "weight": weight, "rgb": rgb}
 
 
+def snapshot_header(snap):
+    """Fields of the vmap_snapshot_header at the start of a snapshot image (a
+    uint8 numpy array, bytes, or a torch uint8 tensor on any device): format,
+    colour, block count and bytes, voxel size, truncation, weight cap, sticky
+    error flags and the key / pool offsets. Raises ValueError on an image
+    that is too short or does not start with the snapshot magic."""
+    size = C.sizeof(L.SnapshotHeader)
+    if isinstance(snap, (bytes, bytearray, memoryview)):
+        raw = bytes(snap[:size])
+    elif isinstance(snap, np.ndarray):
+        raw = snap.reshape(-1).view(np.uint8)[:size].tobytes()
+    else:
+        raw = snap.reshape(-1)[:size].cpu().numpy().tobytes()
+    if len(raw) < size:
+        raise ValueError("a snapshot image holds at least %d bytes, got %d" % (size, len(raw)))
+    h = L.SnapshotHeader.from_buffer_copy(raw)
+    if h.magic != b"VMAPSNAP":
+        raise ValueError("not a snapshot image (magic %r)" % h.magic)
+    return {k: getattr(h, k) for k, _ in L.SnapshotHeader._fields_ if k != "magic"}
+
+
 class HostPipeline:
     """Frames from host memory through vmap_frame_host_async: copies of
     neighbouring frames overlap each other's kernels.
