@@ -1,0 +1,44 @@
+"""bench.py's host-side bookkeeping without a GPU: the clock record taken from
+nvidia-smi samples (busy samples only, throttle reasons by name), percentiles
+and the whole-job throughput."""
+import sys
+from pathlib import Path
+
+import pytest
+
+ROOT = Path(__file__).resolve().parent.parent
+sys.path.insert(0, str(ROOT))
+import bench  # noqa: E402
+
+
+def row(sm, util, hw="Not Active", cap="Not Active", mx=1965):
+    return "0, %s, %s, 512.30, 0x0000000000000000, %s, Not Active, Not Active, %s, %s" % (sm, mx, hw, cap, util)
+
+
+def sampler(lines):
+    c = bench.ClockSampler(None)
+    c.out = "\n".join(lines) + "\n"
+    return c
+
+
+def test_clock_summary_uses_busy_samples_and_names_reasons():
+    lines = [row(345, 0, hw="Active"),  # idle before the timed work: not counted
+             row(1965, 100), row(1965, 98, cap="Active"), row(1950, 100), row(1965, 97),
+             row(400, 3)]
+    s = sampler(lines).summary()
+    assert s["sm_mhz"] == 1965 and s["sm_max_mhz"] == 1965
+    assert s["reasons"] == ["sw_power_cap"]
+    assert s["samples"] == 6 and s["busy_samples"] == 4
+
+
+def test_clock_summary_falls_back_to_all_samples_and_tolerates_missing_values():
+    s = sampler([row(1200, 10), row("[N/A]", 20), row(1300, 30)]).summary()
+    assert s["sm_mhz"] == 1250 and s["busy_samples"] == 0 and s["reasons"] == []
+    assert sampler([]).summary()["reasons"] == ["unavailable"]
+    assert sampler(["garbage"]).summary()["samples"] == 0
+
+
+def test_throughput_and_percentiles():
+    assert bench.job_throughput(200, 100.0, 4) == pytest.approx(4 * 200 / 0.1)
+    assert bench.percentile([1.0, 2.0, 3.0, 4.0], 50) == pytest.approx(2.5)
+    assert bench.percentile([], 99) == 0.0
