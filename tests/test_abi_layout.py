@@ -84,3 +84,31 @@ def test_snapshot_header_reader():
     bad[0] = ord("X")
     with pytest.raises(ValueError):
         snapshot_header(bad)
+
+
+def expected_map_bytes(w, h, num_entries, num_blocks, fmt, color):
+    """Device bytes of one map as documented: hash slots (4 x 16 B per bucket;
+    buckets = int(0.9 numVoxels), raised to cover numEntries), block keys,
+    voxel pool, 16 counters, visible list, near and far z-range tiles (8x8
+    pixels), a triangle counter; each buffer starts on a 256-byte boundary."""
+    nb = max(int(num_blocks * 0.9), 1)
+    nb = max(nb, -(-num_entries // 4))
+    tiles = -(-w // 8) * -(-h // 8)
+    bb = L.lib().vmap_block_bytes(fmt, color)
+    sizes = [nb * 4 * 16, num_blocks * 8, num_blocks * bb, 16 * 4, num_blocks * 4, tiles * 8, tiles * 8, 4]
+    return sum(-(-s // 256) * 256 for s in sizes)
+
+
+@pytest.mark.parametrize("case", [(640, 480, 1 << 21, 1 << 20, L.VOXEL_F32, 1), (320, 240, 0, 1 << 18, L.VOXEL_REF, 0),
+                                  (1280, 720, 1 << 20, 1 << 16, L.VOXEL_F16, 1), (64, 48, 0, 1000, L.VOXEL_I16, 0)])
+def test_required_bytes_matches_the_documented_layout(case):
+    w, h, ne, nb, fmt, color = case
+    cfg = L.Config(width=w, height=h, fx=500.0, fy=500.0, cx=w / 2, cy=h / 2, num_entries=ne, num_blocks=nb,
+                   voxel_size=0.005, num_buckets=0, truncation=0.0, voxel_format=fmt, max_weight=0, with_color=color,
+                   raycast_mode=0)
+    got = C.c_uint64()
+    assert L.lib().vmap_required_bytes(C.byref(cfg), C.byref(got)) == L.VMAP_OK
+    assert got.value == expected_map_bytes(w, h, ne, nb, fmt, color)
+    bad = L.Config(**{k: getattr(cfg, k) for k, _ in L.Config._fields_})
+    bad.voxel_size = 0.0
+    assert L.lib().vmap_required_bytes(C.byref(bad), C.byref(got)) == 1  # VMAP_ERR_INVALID_ARG
