@@ -148,3 +148,70 @@ def test_normals_of_a_planar_vertex_map():
     interior = nm[1:-1, 1:-1, :3].reshape(-1, 3)
     assert np.abs(np.abs(interior @ want) - 1.0).max() < 1e-5
     assert np.isnan(nm[-1]).all() and np.isnan(nm[:, -1]).all()  # last row and column are undefined
+
+
+def restated_blocks(depth, t, R):
+    """Block set of the reference's allocation (depth_fusion.cu:32-59) for a
+    camera with identity rotation at translation t, restated in numpy in the
+    arithmetic type R: band ends floored to voxels, the segment between them
+    sampled at ceil(2 |dir|) points by repeated addition, each sample
+    truncated toward zero (cast<int>) and then mapped voxel -> block."""
+    vs, tdh = R(np.float32(VS)), R(np.float32(VS) * np.float32(4)) * R(0.5)
+    ifx, ify = R(1.0 / np.float64(np.float32(F))), R(1.0 / np.float64(np.float32(F)))
+    cx, cy = R(np.float32(K[0, 2])), R(np.float32(K[1, 2]))
+    y, x = np.mgrid[0:H, 0:W]
+    d = depth.astype(R).ravel()
+    dn = np.maximum(d - tdh, R(0.1))
+    df = np.maximum(d + tdh, R(0.1))
+    ends = []
+    for z in (dn, df):
+        u = np.stack([ifx * (x.ravel().astype(R) - cx) * z, ify * (y.ravel().astype(R) - cy) * z, z], 1).astype(R)
+        w = (np.asarray(t, np.float64).astype(R)[None, :] + u).astype(R)
+        ends.append(np.floor(w / vs).astype(np.int64))
+    pn, pf = ends
+    dirv = (pf - pn).astype(R)
+    n = np.ceil(2.0 * np.sqrt((dirv.astype(np.float64) ** 2).sum(1))).astype(np.int64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        step = (dirv / (n - 1).astype(R)[:, None]).astype(R)
+    pos = pn.astype(R)
+    out = set()
+    for k in range(int(n.max())):
+        live = n > k
+        v = np.trunc(pos[live]).astype(np.int64)
+        q = np.where(v < 0, v - 7, v)
+        b = np.where(q < 0, -((-q) // 8), q // 8)
+        out |= set(map(tuple, b))
+        pos = (pos + step).astype(R)
+    return out
+
+
+@pytest.mark.parametrize("precision", [O.FP32, O.FP64])
+def test_negative_octant_allocation_follows_the_reference_rule(precision):
+    # a wall seen from a camera in the negative octant: the reference truncates
+    # band samples toward zero (cast<int>) where fusion floors
+    # (map_struct.h:111-180), and whether the band's last sample, reached by
+    # repeated addition, lands just above a negative integer decides whether a
+    # second layer of blocks is touched; the oracle must follow that rule in
+    # either arithmetic type
+    R = np.float32 if precision == O.FP32 else np.float64
+    sb = np.array([-25, -20, -38], np.int64)
+    pose = np.eye(4)
+    pose[:3, 3] = sb * 8 * VS
+    depth = np.full((H, W), 1.003, np.float32)  # surface and band ends off the voxel boundaries
+    maps = []
+    for p in (POSE, pose):
+        om = O.OracleMap(W, H, K, 4096, VS, precision=precision, storage="f32", with_color=False)
+        om.fuse(depth, None, p)
+        maps.append(om)
+    k0 = set(map(tuple, maps[0].export()["coords"].astype(np.int64)))
+    k1 = set(map(tuple, maps[1].export()["coords"].astype(np.int64)))
+    assert k0 == restated_blocks(depth, (0, 0, 0), R)
+    want = restated_blocks(depth, pose[:3, 3], R)
+    assert all(min(b) < 0 for b in k1)
+    assert k1 == want  # FP32: 342 blocks in one layer; FP64: 598, the last samples reach z = -22
+    # fusion and ray marching floor, so the surface itself is where it was
+    v0, v1 = maps[0].raycast(POSE), maps[1].raycast(pose)
+    both = np.isfinite(v0[..., 0]) & np.isfinite(v1[..., 0])
+    assert both[4:-4, 4:-4].mean() > 0.95
+    assert np.abs(v1[..., 2][both] - 1.003).max() < 1e-3
+    assert np.abs(v1[..., 2][both] - v0[..., 2][both]).max() < 1e-3
