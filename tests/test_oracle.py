@@ -215,3 +215,17 @@ def test_negative_octant_allocation_follows_the_reference_rule(precision):
     assert both[4:-4, 4:-4].mean() > 0.95
     assert np.abs(v1[..., 2][both] - 1.003).max() < 1e-3
     assert np.abs(v1[..., 2][both] - v0[..., 2][both]).max() < 1e-3
+
+
+def test_full_pool_keeps_its_blocks_and_counts_refusals():
+    full = O.OracleMap(W, H, K, 4096, VS, storage="f32", with_color=False)
+    need = full.fuse(wall(), None, POSE)["new"]
+    om = O.OracleMap(W, H, K, 50, VS, storage="f32", with_color=False)
+    res = om.fuse(wall(), None, POSE)
+    assert need > 50 and res["new"] == 50 and res["failed"] > 0 and om.num_blocks() == 50
+    kept = set(map(tuple, om.export()["coords"]))
+    assert kept <= set(map(tuple, full.export()["coords"]))
+    e = om.export()
+    assert (e["weight"] > 0).any(axis=1).all()  # the blocks it kept are fused
+    res2 = om.fuse(wall(), None, POSE)
+    assert res2["new"] == 0 and res2["failed"] > 0 and set(map(tuple, om.export()["coords"])) == kept
