@@ -229,3 +229,23 @@ def test_full_pool_keeps_its_blocks_and_counts_refusals():
     assert (e["weight"] > 0).any(axis=1).all()  # the blocks it kept are fused
     res2 = om.fuse(wall(), None, POSE)
     assert res2["new"] == 0 and res2["failed"] > 0 and set(map(tuple, om.export()["coords"])) == kept
+
+
+@pytest.mark.parametrize("storage", ["ref", "i16", "f16"])
+def test_wall_tsdf_quantised_like_the_storage_format(storage):
+    om = O.OracleMap(W, H, K, 4096, VS, storage=storage, with_color=False)
+    om.fuse(wall(), None, POSE)
+    e = om.export()
+    loc = np.arange(512)
+    z = (e["coords"][:, 2:3] * 8 + (loc // 64)[None, :]) * VS
+    obs = e["weight"] > 0
+    want = np.minimum(1.0, (D - z) / MU)[obs]
+    got = e["tsdf"][obs]
+    if storage == "f16":
+        # IEEE half, round to nearest even
+        assert np.array_equal(got, want.astype(np.float16).astype(np.float64))
+    else:
+        # int16 x 32767, truncated toward zero (packFloat, map_struct.h:72-80)
+        codes = np.round(got * 32767)
+        assert np.abs(got * 32767 - codes).max() < 1e-3
+        assert np.array_equal(codes, np.trunc(want * 32767))
