@@ -249,3 +249,11 @@ def test_wall_tsdf_quantised_like_the_storage_format(storage):
         codes = np.round(got * 32767)
         assert np.abs(got * 32767 - codes).max() < 1e-3
         assert np.array_equal(codes, np.trunc(want * 32767))
+
+
+def test_sixteen_bit_weights_cap_above_255():
+    om = O.OracleMap(W, H, K, 4096, VS, storage="i16", max_weight=260, with_color=False)
+    for _ in range(262):
+        om.fuse(wall(), None, POSE)
+    w = om.export()["weight"]
+    assert w.max() == 260 and set(np.unique(w)) <= {0.0, 260.0}
