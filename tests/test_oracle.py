@@ -257,3 +257,22 @@ def test_sixteen_bit_weights_cap_above_255():
         om.fuse(wall(), None, POSE)
     w = om.export()["weight"]
     assert w.max() == 260 and set(np.unique(w)) <= {0.0, 260.0}
+
+
+@pytest.mark.parametrize("precision", [O.FP32, O.FP64])
+def test_sphere_mesh_lies_on_the_surface_with_outward_normals(precision):
+    center, radius = np.array([0.05, -0.03, 1.2]), 0.35
+    om = O.OracleMap(W, H, K, 8192, VS, precision=precision, storage="f32", with_color=False)
+    om.fuse(np.nan_to_num(sphere_depth(center, radius), nan=0.0), None, POSE)
+    n, verts, norms = om.polygonize()
+    assert n > 1000
+    p = verts.reshape(-1, 3).astype(np.float64)
+    r = np.linalg.norm(p - center, axis=1)
+    radial = (p - center) / r[:, None]
+    facing = (radial * -p / np.linalg.norm(p, axis=1)[:, None]).sum(1) > 0.9  # the cap facing the camera
+    assert facing.mean() > 0.05
+    # one 64x48 frame: a pixel covers 2.5 voxels at 1 m and each voxel takes its nearest pixel's depth
+    assert np.abs(r[facing] - radius).max() < 0.5 * VS
+    assert np.abs(r - radius).max() < 1.5 * VS  # grazing rim included
+    # face normals point out of the surface, into the observed free space (TSDF > 0)
+    assert ((norms.reshape(-1, 3) * radial).sum(1) > 0).all()
