@@ -73,6 +73,17 @@ def max_over_ranks(x, device, world):
     return float(t.item())
 
 
+def all_gather_objects(x, world):
+    """Every rank's x, in rank order: one all_gather_object (control data only,
+    e.g. free device memory or summaries); [x] on one rank."""
+    if world == 1:
+        return [x]
+    import torch.distributed as dist
+    out = [None] * world
+    dist.all_gather_object(out, x)
+    return out
+
+
 def job_throughput(units_per_rank, max_total_ms, world):
     """Whole-job units per second: every rank processed units_per_rank units
     within the slowest rank's max_total_ms."""
@@ -716,18 +727,23 @@ def run_product(args):
     if args.serving:
         from voxelmapping_b200 import serving as S
         rates = [float(r) for r in args.serving_rates.split(",")]
-        line["serving"] = {"config": "256 sessions of uneven extent / voxel size / resolution (FP16 + colour), 4 "
-                                     "pre-rendered frames each in pinned host memory; Poisson arrivals at each offered "
-                                     "rate, %d requests, 70/25/5 fuse/raycast/mesh; raycasts return vertex + normal "
-                                     "maps to pinned host memory, meshes their triangles; latency = completion - "
-                                     "arrival, wall clock" % args.serving_requests, "runs": []}
+        line["serving"] = {"config": "256 sessions per GPU of uneven extent / voxel size / resolution (FP16 + "
+                                     "colour; with N GPUs the job's N x 256 sessions are partitioned over them by free "
+                                     "device memory), 4 pre-rendered frames each in pinned host memory; Poisson "
+                                     "arrivals at each offered rate per GPU, %d requests per GPU, 70/25/5 "
+                                     "fuse/raycast/mesh; raycasts return vertex + normal maps to pinned host memory, "
+                                     "meshes their triangles; latency = completion - arrival, wall clock; summaries "
+                                     "merged over the ranks" % args.serving_requests, "runs": []}
+        gather = lambda x: all_gather_objects(x, world)  # noqa: E731
         for frac in [float(b) for b in args.serving_budgets.split(",")]:
             res, ex = S.run_serving(n_sessions=256, rates=rates, count=args.serving_requests, budget_frac=frac,
-                                    warmup=500, seed=rank)
+                                    warmup=500, seed=0, rank=rank, world=world, all_gather=gather)
             ex.release()
-            for r in res:
+            parts = gather(res)
+            for k in range(len(res)):
+                r = S.merge_summaries([p[k] for p in parts])
                 r["budget_frac"] = frac
-                line["serving"]["runs"].append({k: v for k, v in r.items() if not k.startswith("_")})
+                line["serving"]["runs"].append({key: v for key, v in r.items() if not key.startswith("_")})
     if rank == 0:
         print(json.dumps(line), flush=True)
     vm.release()

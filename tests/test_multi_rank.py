@@ -69,3 +69,54 @@ def test_reference_arm_runs_on_rank_zero_only(monkeypatch):
     class A:
         warmup, steps, gpus = 1, 1, 2
     assert bench.run_reference(A) is None  # returns at once, prints nothing
+
+
+def _serve_rank(rank, world, port, out):
+    """One rank of a served job: capacities shared with bench.all_gather_objects,
+    sessions partitioned, this rank's requests served (fake executor, simulated
+    clock), summaries gathered and merged."""
+    sys.path.insert(0, str(ROOT))
+    sys.path.insert(0, str(ROOT / "tests"))
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    from datetime import timedelta
+
+    import numpy as np
+    import torch.distributed as dist
+    import bench
+    from test_serving_host import FakeExecutor
+    from voxelmapping_b200 import serving as S
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        sizes = [int(x) for x in np.random.default_rng(0).integers(1, 20, 64) * 1000]  # the job's sessions
+        caps = bench.all_gather_objects([3e5, 1e5][rank], world)  # each rank's free memory
+        owner = S.partition_sessions(sizes, caps)
+        reqs = S.poisson_requests(64, 1e9, 2000, seed=1)
+        loc, mine = S.local_requests(reqs, owner, rank)
+        lsizes = [sizes[s] for s in mine]
+        sched = S.Scheduler(lsizes, sum(lsizes), max_mesh_per_tick=2)
+        ex = FakeExecutor(sched)
+        done, stats = S.serve(loc, sched, ex, clock=lambda: ex.t,
+                              wait_until=lambda t: setattr(ex, "t", max(ex.t, t)))
+        merged = S.merge_summaries(bench.all_gather_objects(S.summarize(done, stats), world))
+        out.put((rank, caps, owner, mine, sum(lsizes), merged["requests"], merged["ranks"], merged["all"]["n"]))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_two_gloo_ranks_partition_sessions_by_free_memory_and_merge_serving_summaries():
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_serve_rank, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, caps0, own0, mine0, held0, n0, k0, a0), (_, caps1, own1, mine1, held1, n1, k1, a1) = res
+    assert caps0 == caps1 == [3e5, 1e5] and own0 == own1
+    assert not set(mine0) & set(mine1) and sorted(mine0 + mine1) == list(range(64))
+    assert held0 > held1  # the rank with more free memory holds more of the sessions' bytes
+    assert n0 == n1 == 2000 and k0 == k1 == 2 and a0 == a1 == 2000

@@ -239,3 +239,64 @@ def test_mesh_worker_that_cannot_start_fails_its_requests():
     _submit(ex, reqs, T.perf_counter)
     with pytest.raises(RuntimeError, match="mesh worker stopped"):
         ex.inflight()
+
+
+# -- several GPUs: partition, routing and merging ------------------------------
+def test_partition_follows_capacity_and_balances_bytes():
+    rng = np.random.default_rng(3)
+    sizes = [int(x) for x in rng.integers(1, 50, 512) * 1000]
+    for caps in ([1e6] * 4, [4e6, 2e6, 1e6, 1e6]):
+        owner = S.partition_sessions(sizes, caps)
+        assert len(owner) == len(sizes) and set(owner) == set(range(len(caps)))
+        held = [sum(b for b, r in zip(sizes, owner) if r == k) for k in range(len(caps))]
+        left = [c - h for c, h in zip(caps, held)]
+        assert max(left) - min(left) <= max(sizes)
+        assert owner == S.partition_sessions(sizes, caps)  # deterministic
+    assert S.partition_sessions(sizes, [1.0]) == [0] * len(sizes)
+    with pytest.raises(ValueError):
+        S.partition_sessions(sizes, [])
+
+
+def test_local_requests_split_the_stream_by_owner():
+    reqs = S.poisson_requests(10, 1000.0, 500, seed=4)
+    owner = [s % 3 for s in range(10)]
+    seen = []
+    for rank in range(3):
+        loc, mine = S.local_requests(reqs, owner, rank)
+        assert mine == [s for s in range(10) if s % 3 == rank]
+        assert [r.index for r in loc] == list(range(len(loc)))
+        assert all(a.arrival <= b.arrival for a, b in zip(loc, loc[1:]))
+        seen += [(mine[r.session], r.kind, r.arrival) for r in loc]
+    assert sorted(seen) == sorted((r.session, r.kind, r.arrival) for r in reqs)
+
+
+def _summary(n_sessions, seed, makespan_scale=1.0):
+    out, stats, _ = run(n_sessions, 1e9, 400, 1.0, seed=seed)
+    stats["makespan_s"] *= makespan_scale
+    return S.summarize(out, stats)
+
+
+def test_merge_summaries():
+    one = _summary(8, 0)
+    m = S.merge_summaries([one])
+    assert m["ranks"] == 1 and all(m[k] == one[k] for k in one)
+    a, b = _summary(8, 1), _summary(8, 2, makespan_scale=2.0)
+    for p in (a, b):
+        p.update(offered_rps=100.0, sessions=8, budget_gb=1.0, all_sessions_gb=1.0)
+    m = S.merge_summaries([a, b])
+    assert m["ranks"] == 2 and m["requests"] == 800 and m["sessions"] == 16 and m["offered_rps"] == 200.0
+    assert m["makespan_s"] == max(a["makespan_s"], b["makespan_s"])
+    assert m["throughput_rps"] == pytest.approx(800 / m["makespan_s"])
+    lat = a["_latencies"]["all"] + b["_latencies"]["all"]
+    assert m["all"]["n"] == 800 and m["all"]["p99_ms"] == pytest.approx(1e3 * np.percentile(lat, 99))
+    assert m["evictions"] == a["evictions"] + b["evictions"] and len(m["per_rank"]) == 2
+
+
+def test_session_bytes_is_the_map_plus_its_image_buffers():
+    from voxelmapping_b200 import synth
+    from voxelmapping_b200.vmapping import VoxelMapping
+    for w in synth.uneven_workloads(6, seed=5):
+        vm = VoxelMapping(w.width, w.height, w.K, voxel_format=w.voxel_format, with_color=w.with_color,
+                          max_weight=w.max_weight)
+        assert S.session_bytes(w) == vm.required_bytes(w.num_entries, w.num_blocks, w.voxel_size) + \
+            w.width * w.height * 37

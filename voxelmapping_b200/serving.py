@@ -287,10 +287,8 @@ class GpuExecutor:
         return self._new_map(s).required_bytes(w.num_entries, w.num_blocks, w.voxel_size)
 
     def session_bytes(self, s):
-        """Device bytes of session s while resident: its map
-        (vmap_required_bytes) plus its frame and vertex / normal map buffers."""
-        w = self.wls[s]
-        return self.map_bytes(s) + w.width * w.height * (2 + 3 + 16 + 16)
+        """Device bytes of session s while resident (session_bytes)."""
+        return session_bytes(self.wls[s])
 
     def restore(self, s):
         torch = self.torch
@@ -500,15 +498,85 @@ def serve(requests, scheduler, executor, clock=None, wait_until=None, stall_s=12
     return requests, stats
 
 
+def _latency_stats(lat):
+    return {"n": len(lat), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
+            "p99_ms": 1e3 * float(np.percentile(lat, 99)), "mean_ms": 1e3 * float(np.mean(lat))}
+
+
 def summarize(requests, stats):
-    """Throughput and latency percentiles (ms) per request kind."""
-    out = {"requests": len(requests), "throughput_rps": len(requests) / stats["makespan_s"]}
+    """Throughput and latency percentiles (ms) per request kind; the raw
+    latencies (seconds) per kind stay under "_latencies" for merge_summaries."""
+    out = {"requests": len(requests), "throughput_rps": len(requests) / stats["makespan_s"], "_latencies": {}}
     for kind in KINDS + ("all",):
         lat = [r.latency for r in requests if kind in ("all", r.kind)]
         if lat:
-            out[kind] = {"n": len(lat), "p50_ms": 1e3 * float(np.percentile(lat, 50)),
-                         "p99_ms": 1e3 * float(np.percentile(lat, 99)), "mean_ms": 1e3 * float(np.mean(lat))}
+            out[kind] = _latency_stats(lat)
+            out["_latencies"][kind] = lat
     out.update(stats)
+    return out
+
+
+# -- several GPUs: sessions are independent, so they are partitioned ----------
+def session_bytes(w):
+    """Device bytes of a session with workload w while resident: its map
+    (vmap_required_bytes, computed on the host) plus its frame and vertex /
+    normal map buffers."""
+    from .vmapping import VoxelMapping
+    vm = VoxelMapping(w.width, w.height, w.K, voxel_format=w.voxel_format, with_color=w.with_color,
+                      max_weight=w.max_weight)
+    return vm.required_bytes(w.num_entries, w.num_blocks, w.voxel_size) + w.width * w.height * (2 + 3 + 16 + 16)
+
+
+def partition_sessions(sizes, capacities):
+    """Session -> rank. Sessions in decreasing size (ties by index), each to
+    the rank with the most bytes left (its capacity, e.g. free device memory,
+    minus the sessions it already holds; ties to the lower rank). Each rank's
+    share of the bytes then follows its capacity: the bytes left differ by at
+    most one session's size. Capacities may be exceeded; the ranks then evict."""
+    if not capacities:
+        raise ValueError("no ranks to place sessions on")
+    left = [float(c) for c in capacities]
+    owner = [0] * len(sizes)
+    for s in sorted(range(len(sizes)), key=lambda s: (-sizes[s], s)):
+        r = max(range(len(left)), key=lambda r: (left[r], -r))
+        owner[s] = r
+        left[r] -= sizes[s]
+    return owner
+
+
+def local_requests(requests, owner, rank):
+    """The requests addressed to the sessions that `owner` gives `rank`, with
+    sessions renumbered to that rank's list (global order) and indices to the
+    order of arrival. Returns (requests, global session ids of the rank)."""
+    mine = [s for s, r in enumerate(owner) if r == rank]
+    local = {s: i for i, s in enumerate(mine)}
+    out = []
+    for q in requests:
+        if q.session in local:
+            out.append(Request(q.kind, local[q.session], q.arrival, len(out)))
+    return out, mine
+
+
+def merge_summaries(parts):
+    """One job-level summary from the per-rank summaries of the same run:
+    requests, offered rates, sessions, budgets and eviction counters add up;
+    throughput is all requests over the slowest rank's makespan; percentiles
+    are over every rank's latencies ("_latencies"). Per-rank tick statistics
+    stay under "per_rank". A single part comes back unchanged."""
+    if len(parts) == 1:
+        return dict(parts[0], ranks=1)
+    out = {"ranks": len(parts), "requests": sum(p["requests"] for p in parts),
+           "makespan_s": max(p["makespan_s"] for p in parts)}
+    out["throughput_rps"] = out["requests"] / out["makespan_s"]
+    for kind in KINDS + ("all",):
+        lat = [x for p in parts for x in p.get("_latencies", {}).get(kind, [])]
+        if lat:
+            out[kind] = _latency_stats(lat)
+    for k in ("offered_rps", "sessions", "budget_gb", "all_sessions_gb", "evictions", "restores"):
+        if all(k in p for p in parts):
+            out[k] = sum(p[k] for p in parts)
+    out["per_rank"] = [{k: p[k] for k in ("requests", "makespan_s", "ticks", "mean_batch", "busy_s", "sessions")
+                        if k in p} for p in parts]
     return out
 
 
@@ -532,21 +600,38 @@ def render_frames(workloads, n_frames, pin=True):
 
 
 def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, budget_frac=0.5, n_frames=4,
-                seed=0, warmup=500, max_mesh_per_tick=2, keep_results=False, pool_scale=1, log=None):
+                seed=0, warmup=500, max_mesh_per_tick=2, keep_results=False, pool_scale=1, log=None,
+                rank=0, world=1, all_gather=None):
     """Builds n_sessions uneven sessions (FP16 + colour), then for each rate
     replays `count` Poisson requests (70/25/5 fuse/raycast/mesh) after a
     warm-up that touches every session and `warmup` more requests. The
     budget is `budget_bytes`, or
     `budget_frac` of all sessions' bytes, capped at 85 % of the free device
-    memory. `pool_scale` multiplies every pool. Returns (list of per-rate
-    summaries, executor)."""
+    memory. `pool_scale` multiplies every pool.
+
+    With world > 1 ranks (one process per GPU) the job holds n_sessions x
+    world sessions, partitioned over the ranks by free device memory
+    (partition_sessions; `all_gather(x)` returns every rank's x in rank
+    order); rate and request count scale by world and every rank serves the
+    requests of its own sessions, so the work per GPU stays that of one rank
+    alone. merge_summaries combines the ranks' summaries. Returns (list of
+    this rank's per-rate summaries, executor)."""
     import torch
     from . import synth
-    wls = [dataclasses.replace(w, num_blocks=w.num_blocks * pool_scale)
-           for w in synth.uneven_workloads(n_sessions, seed=seed)]
+    total = n_sessions * world
+    all_wls = [dataclasses.replace(w, num_blocks=w.num_blocks * pool_scale)
+               for w in synth.uneven_workloads(total, seed=seed)]
+    owner = [0] * total
+    if world > 1:
+        free, _ = torch.cuda.mem_get_info()
+        owner = partition_sessions([session_bytes(w) for w in all_wls], all_gather(free))
+    wls = [all_wls[s] for s in range(total) if owner[s] == rank]
+    n_local = len(wls)
+    if n_local == 0:
+        raise ValueError("rank %d holds no session" % rank)
     frames = render_frames(wls, n_frames)
     ex = GpuExecutor(wls, frames, keep_results=keep_results)
-    sizes = [ex.session_bytes(s) for s in range(n_sessions)]
+    sizes = [ex.session_bytes(s) for s in range(n_local)]
     free, _ = torch.cuda.mem_get_info()
     budget = int(budget_bytes or budget_frac * sum(sizes))
     budget = max(max(sizes), min(budget, int(0.85 * free)))
@@ -562,18 +647,20 @@ def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, 
             # size), then `warmup` requests at the highest rate: first-touch
             # costs stay out of the measured runs
             for _ in range(max(2, n_frames)):
-                serve([Request(k, s, 0.0, 0) for s in range(n_sessions) for k in ("fuse", "raycast")], sched, ex)
-            big = sorted(range(n_sessions), key=lambda s: -wls[s].num_blocks)[:16]
+                serve([Request(k, s, 0.0, 0) for s in range(n_local) for k in ("fuse", "raycast")], sched, ex)
+            big = sorted(range(n_local), key=lambda s: -wls[s].num_blocks)[:16]
             serve([Request("mesh", s, 0.0, 0) for s in big], sched, ex)
-            serve(poisson_requests(n_sessions, max(rates), warmup, seed=seed + 7), sched, ex)
+            serve(poisson_requests(n_local, max(rates), warmup, seed=seed + 7), sched, ex)
         for k, rate in enumerate(rates):
             sched.evictions = sched.restores = 0
-            reqs = poisson_requests(n_sessions, rate, count, seed=seed + 100 + k)
+            reqs = poisson_requests(total, rate * world, count * world, seed=seed + 100 + k)
+            if world > 1:
+                reqs, _ = local_requests(reqs, owner, rank)
             ex.phase.clear()
             reqs, stats = serve(reqs, sched, ex)
             summ = summarize(reqs, stats)
             summ["phase_s"] = {k: round(v, 4) for k, v in ex.phase.items()}
-            summ.update({"offered_rps": rate, "sessions": n_sessions, "budget_gb": budget / 1e9,
+            summ.update({"offered_rps": rate * world * n_local / total, "sessions": n_local, "budget_gb": budget / 1e9,
                          "all_sessions_gb": sum(sizes) / 1e9})
             results.append(summ)
             if log:
