@@ -1,4 +1,4 @@
-"""Serving many mapping sessions from one GPU.
+"""Serving many mapping sessions from one GPU or several.
 
 A session is one map (its own scene, camera, voxel size and pool). Requests
 arrive over time: "fuse" (a depth + colour frame to integrate), "raycast"
@@ -22,6 +22,12 @@ admitted if its bytes fit the budget, evicting least-recently-used idle
 sessions (snapshot to pinned host memory, map released) as needed; if they
 still do not fit, its requests wait. At most VMAP_MAX_BATCH (256) maps are
 resident, the batch step's limit.
+
+On several GPUs (one process per GPU) sessions stay independent: they are
+partitioned over the ranks by free device memory (partition_sessions), every
+rank serves the requests of its own sessions (local_requests) with its own
+scheduler and executor, and only control data crosses ranks: the free-memory
+figures before and the summaries after (merge_summaries).
 
 `Scheduler` is pure host logic (tested on the CPU with a fake executor);
 `GpuExecutor` drives the library.
