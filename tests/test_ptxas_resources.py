@@ -1,0 +1,35 @@
+"""Kernel resources as ptxas reports them (no GPU): the ray marcher fits the
+64 registers that 4 resident CTAs of 256 threads per SM leave it
+(__launch_bounds__(256, 4)) with a small spill, the other kernels spill at
+most a few words, and no kernel needs more static shared memory than the
+48 KB a launch gets without opting in."""
+import pytest
+
+from voxelmapping_b200 import build as B
+
+
+@pytest.fixture(scope="module")
+def report():
+    return B.ptxas_report()
+
+
+def test_every_kernel_is_reported(report):
+    names = " ".join(report)
+    for k in ("alloc_kernel", "visibility_kernel", "fuse_kernel", "zrange_kernel", "raycast_kernel",
+              "normals_kernel", "mesh_kernel", "phong_kernel", "export_kernel"):
+        assert k in names, k
+    assert all(r["registers"] > 0 for r in report.values())
+
+
+def test_ray_marcher_fits_four_ctas_per_sm(report):
+    rm = {k: r for k, r in report.items() if "raycast_kernel" in k}
+    assert len(rm) == 8  # one view or many, four voxel formats
+    for k, r in rm.items():
+        assert r["registers"] <= 64 and r["spill_stores"] <= 128, (k, r)
+
+
+def test_other_kernels_barely_spill_and_fit_default_shared_memory(report):
+    for k, r in report.items():
+        if "raycast_kernel" not in k:
+            assert r["spill_stores"] <= 32, (k, r)
+        assert r["smem"] <= 48 * 1024, (k, r)

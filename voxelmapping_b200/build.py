@@ -57,7 +57,7 @@ def _run(cmd, verbose):
     return r
 
 
-def build(verbose=False, ptxas_info=False):
+def build(verbose=False):
     OBJ.mkdir(exist_ok=True)
     hdrs = _headers()
     jobs = []
@@ -67,12 +67,9 @@ def build(verbose=False, ptxas_info=False):
         o = OBJ / (src + ".o")
         objs.append(o)
         if _stale(o, [s] + hdrs):
-            extra = ["-Xptxas", "-v"] if ptxas_info else []
-            jobs.append([nvcc()] + NVCC_FLAGS + extra + ["-c", s, "-o", o])
+            jobs.append([nvcc()] + NVCC_FLAGS + ["-c", s, "-o", o])
     with cf.ThreadPoolExecutor(max_workers=len(CUDA_SOURCES)) as ex:
-        for r in ex.map(lambda c: _run(c, verbose), jobs):
-            if ptxas_info:
-                print(r.stderr)
+        list(ex.map(lambda c: _run(c, verbose), jobs))
     if _stale(LIB, objs):
         _run([nvcc()] + ARCH + ["-shared", "-o", LIB] + objs + ["-lcudart_static", "-lrt", "-lpthread", "-ldl"],
              verbose)
@@ -83,6 +80,45 @@ def build(verbose=False, ptxas_info=False):
     return LIB
 
 
+def ptxas_report(sources=("raymarch.cu", "fusion.cu", "mesh.cu", "raycast.cu", "batch.cu", "export_static.cu",
+                           "snapshot.cu", "map.cu")):
+    """Per-kernel resources as ptxas reports them (-Xptxas -v) for the given
+    CUDA sources, compiled with the library's flags into a temporary
+    directory: {kernel (demangled): {"registers", "spill_stores",
+    "spill_loads", "stack", "smem"}}."""
+    import re
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        cmds = [[nvcc()] + NVCC_FLAGS + ["-Xptxas", "-v", "-c", CSRC / src, "-o", Path(tmp) / (src + ".o")]
+                for src in sources]
+        with cf.ThreadPoolExecutor(max_workers=len(cmds)) as ex:
+            text = "".join(r.stderr + r.stdout for r in ex.map(lambda c: _run(c, False), cmds))
+    out, cur = {}, None
+    for line in text.splitlines():
+        m = re.search(r"Compiling entry function '([^']+)'", line)
+        if m:
+            cur = m.group(1)
+            out[cur] = {"registers": 0, "spill_stores": 0, "spill_loads": 0, "stack": 0, "smem": 0}
+            continue
+        if cur is None:
+            continue
+        m = re.search(r"(\d+) bytes stack frame, (\d+) bytes spill stores, (\d+) bytes spill loads", line)
+        if m:
+            out[cur].update(stack=int(m.group(1)), spill_stores=int(m.group(2)), spill_loads=int(m.group(3)))
+        m = re.search(r"Used (\d+) registers", line)
+        if m:
+            out[cur]["registers"] = int(m.group(1))
+            sm = re.search(r"(\d+) bytes smem", line)
+            out[cur]["smem"] = int(sm.group(1)) if sm else 0
+    names = list(out)
+    filt = shutil.which("c++filt")
+    if filt and names:
+        dem = subprocess.run([filt], input="\n".join(names), capture_output=True, text=True).stdout.splitlines()
+        if len(dem) == len(names):
+            return {d: out[n] for n, d in zip(names, dem)}
+    return out
+
+
 def build_oracle(verbose=False):
     """Compile the CPU oracle (test infrastructure) with its Makefile."""
     _run(["make", "-s", "-C", ROOT / "oracle", "CC=" + ("/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc")],
@@ -91,5 +127,12 @@ def build_oracle(verbose=False):
 
 
 if __name__ == "__main__":
-    build(verbose=True, ptxas_info="--ptxas" in sys.argv)
-    build_oracle(verbose=True)
+    if "--ptxas" in sys.argv:  # resource table of every kernel, no build
+        print("| kernel | registers | spill stores / loads (B) | stack (B) | static smem (B) |")
+        print("|---|---:|---:|---:|---:|")
+        for k, r in sorted(ptxas_report().items()):
+            print("| `%s` | %d | %d / %d | %d | %d |" % (k.replace("vmapb::", ""), r["registers"], r["spill_stores"],
+                                                     r["spill_loads"], r["stack"], r["smem"]))
+    else:
+        build(verbose=True)
+        build_oracle(verbose=True)
