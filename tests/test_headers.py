@@ -44,3 +44,18 @@ def test_cpp_drop_in_program_links(tmp_path):
                         "-L" + str(lib.parent), "-lvmap_b200", "-L" + str(CUDA / "lib64"), "-lcudart"],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_integration_cpp_snippet_compiles(tmp_path):
+    """The C++ example in INTEGRATION.md uses the class as declared: its body,
+    with the caller's buffers and pose as parameters, compiles."""
+    text = (ROOT / "INTEGRATION.md").read_text()
+    block = text.split("```cpp", 1)[1].split("```", 1)[0]
+    body = "\n".join(l for l in block.splitlines() if not l.lstrip().startswith("#include"))
+    src = tmp_path / "snippet.cpp"
+    src.write_text('#include "vmapping.h"\n'
+                   "void snippet(void* depth_dev, const unsigned char* rgb_host, const float* depth_host,\n"
+                   "             const vmap::Mat4f& cam_to_world) {\n" + body + "\n(void)n; (void)points;\n}\n")
+    r = subprocess.run([compiler("g++"), "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I" + str(ROOT / "include"),
+                        str(src)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
