@@ -60,7 +60,7 @@ typedef enum vmap_status {
  * uint8 weight, map_struct.h:17-21); F32 is the plain single-precision map;
  * F16 / I16 are the reduced-precision formats with uint16 weights. */
 typedef enum vmap_voxel_format {
-    VMAP_VOXEL_REF = 0, /* int16 tsdf, uint8 weight   : 3 B/voxel (+3 colour) */
+    VMAP_VOXEL_REF = 0, /* int16 tsdf, uint8 weight   : 4 B/voxel, 3 used (+3 colour) */
     VMAP_VOXEL_F32 = 1, /* float tsdf, float weight   : 8 B/voxel (+3 colour) */
     VMAP_VOXEL_F16 = 2, /* half tsdf, uint16 weight   : 4 B/voxel (+3 colour) */
     VMAP_VOXEL_I16 = 3  /* int16 tsdf, uint16 weight  : 4 B/voxel (+3 colour) */
