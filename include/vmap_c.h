@@ -277,7 +277,9 @@ vmap_status vmap_set_launch_config(vmap_map* map, const vmap_launch_config* cfg)
 vmap_status vmap_batch_get_launch_config(const vmap_batch* batch, vmap_launch_config* out);
 vmap_status vmap_batch_set_launch_config(vmap_batch* batch, const vmap_launch_config* cfg);
 
-/* ---- inspection ---------------------------------------------------------- */
+/* ---- inspection (no counterpart in the reference: it reports no counters,
+ * and its SafeCall, src/cuda_utils.h:11-26, ends the process on a CUDA
+ * error while capacity failures pass silently) -------------------------------- */
 /* Synchronises `stream`, then reads the device counters. */
 vmap_status vmap_get_stats(vmap_map* map, void* stream, vmap_stats* out);
 vmap_status vmap_clear_errors(vmap_map* map, void* stream);
@@ -377,7 +379,9 @@ vmap_status vmap_timing_enable(vmap_map* map, uint32_t max_records);
 vmap_status vmap_timing_read(vmap_map* map, double ms[VMAP_NUM_STAGES], uint32_t launches[VMAP_NUM_STAGES]);
 
 /* ---- utilities ----------------------------------------------------------- */
-/* The library's pose inverse (FP64, affine), exposed for parity tests. */
+/* The library's pose inverse (FP64, affine), exposed for parity tests; it
+ * replaces the reference's camToWorld.inverse() in float
+ * (src/depth_fusion.cu:251, src/ray_tracing.cu:414). */
 void vmap_pose_inverse(const double pose[16], double inv[16]);
 /* hash (map_struct.h:104-109), exposed for parity tests. */
 int vmap_block_hash(int x, int y, int z, int n_buckets);
