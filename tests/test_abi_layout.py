@@ -112,3 +112,9 @@ def test_required_bytes_matches_the_documented_layout(case):
     bad = L.Config(**{k: getattr(cfg, k) for k, _ in L.Config._fields_})
     bad.voxel_size = 0.0
     assert L.lib().vmap_required_bytes(C.byref(bad), C.byref(got)) == 1  # VMAP_ERR_INVALID_ARG
+
+
+def test_integration_guide_names_every_entry_point():
+    guide = (ROOT / "INTEGRATION.md").read_text()
+    missing = [n for n in declarations() if n not in guide]
+    assert not missing, missing
