@@ -245,16 +245,21 @@ def test_mesh_worker_that_cannot_start_fails_its_requests():
 def test_partition_follows_capacity_and_balances_bytes():
     rng = np.random.default_rng(3)
     sizes = [int(x) for x in rng.integers(1, 50, 512) * 1000]
-    for caps in ([1e6] * 4, [4e6, 2e6, 1e6, 1e6]):
+    # capacities far above, near and below the sessions' total (12.8 MB)
+    for caps in ([1e6] * 4, [4e6, 2e6, 1e6, 1e6], [80e9, 40e9], [8e9] * 8, [3e5, 1e5]):
         owner = S.partition_sessions(sizes, caps)
         assert len(owner) == len(sizes) and set(owner) == set(range(len(caps)))
         held = [sum(b for b, r in zip(sizes, owner) if r == k) for k in range(len(caps))]
-        left = [c - h for c, h in zip(caps, held)]
-        assert max(left) - min(left) <= max(sizes)
+        fill = [h / c for h, c in zip(held, caps)]
+        assert max(fill) - min(fill) <= max(sizes) / min(caps), caps
         assert owner == S.partition_sessions(sizes, caps)  # deterministic
+    owner = S.partition_sessions(sizes, [80e9, 40e9])
+    held = [sum(b for b, r in zip(sizes, owner) if r == k) for k in range(2)]
+    assert abs(held[0] / held[1] - 2.0) < 0.05  # shares follow free memory
     assert S.partition_sessions(sizes, [1.0]) == [0] * len(sizes)
-    with pytest.raises(ValueError):
-        S.partition_sessions(sizes, [])
+    for bad in ([], [1e6, 0]):
+        with pytest.raises(ValueError):
+            S.partition_sessions(sizes, bad)
 
 
 def test_local_requests_split_the_stream_by_owner():
@@ -300,3 +305,50 @@ def test_session_bytes_is_the_map_plus_its_image_buffers():
                           max_weight=w.max_weight)
         assert S.session_bytes(w) == vm.required_bytes(w.num_entries, w.num_blocks, w.voxel_size) + \
             w.width * w.height * 37
+
+
+class FakeGpuExecutor:
+    """Stands in for GpuExecutor inside run_serving: completes every request
+    at once on the wall clock (no device)."""
+
+    def __init__(self, wls, frames, keep_results=False):
+        import collections
+        self.wls, self.frames = wls, frames
+        self.phase = collections.Counter()
+        self.ticks = 0
+
+    def session_bytes(self, s):
+        return S.session_bytes(self.wls[s])
+
+    def run_tick(self, plan, clock):
+        self.ticks += 1
+        for r in plan.requests():
+            r.done = clock()
+
+    def inflight(self):
+        return frozenset()
+
+    def release(self):
+        pass
+
+
+@pytest.mark.parametrize("world", [1, 2])
+def test_run_serving_drives_its_executor_for_each_rank(monkeypatch, world):
+    import torch
+    monkeypatch.setattr(S, "GpuExecutor", FakeGpuExecutor)
+    monkeypatch.setattr(S, "render_frames", lambda wls, n: [[None] * n for _ in wls])
+    monkeypatch.setattr(torch.cuda, "mem_get_info", lambda *a: (80 << 30, 180 << 30))
+    caps = [80 << 30, 40 << 30][:world]
+    per_rank = []
+    for rank in range(world):
+        res, ex = S.run_serving(n_sessions=6, rates=(2000.0,), count=60, budget_frac=1.0, n_frames=2, warmup=10,
+                                seed=3, rank=rank, world=world, all_gather=lambda x: caps)
+        assert len(res) == 1 and ex.ticks > 0
+        per_rank.append(res[0])
+    m = S.merge_summaries(per_rank)
+    assert m["requests"] == 60 * world and m["sessions"] == 6 * world
+    assert m["offered_rps"] == pytest.approx(2000.0 * world)
+    if world == 1:
+        assert per_rank[0]["offered_rps"] == 2000.0 and per_rank[0]["sessions"] == 6
+    else:
+        assert per_rank[0]["sessions"] > per_rank[1]["sessions"]  # twice the free memory

@@ -535,18 +535,19 @@ def session_bytes(w):
 
 def partition_sessions(sizes, capacities):
     """Session -> rank. Sessions in decreasing size (ties by index), each to
-    the rank with the most bytes left (its capacity, e.g. free device memory,
-    minus the sessions it already holds; ties to the lower rank). Each rank's
-    share of the bytes then follows its capacity: the bytes left differ by at
-    most one session's size. Capacities may be exceeded; the ranks then evict."""
-    if not capacities:
-        raise ValueError("no ranks to place sessions on")
-    left = [float(c) for c in capacities]
+    the rank whose fill (bytes held / capacity, e.g. its free device memory)
+    is lowest once it takes the session (ties to the lower rank). Each rank's
+    share of the bytes then follows its capacity, however small the sessions
+    are against it: fills differ by at most one session's size over the
+    smallest capacity. Capacities may be exceeded; the ranks then evict."""
+    if not capacities or min(capacities) <= 0:
+        raise ValueError("every rank needs a positive capacity")
+    held = [0.0] * len(capacities)
     owner = [0] * len(sizes)
     for s in sorted(range(len(sizes)), key=lambda s: (-sizes[s], s)):
-        r = max(range(len(left)), key=lambda r: (left[r], -r))
+        r = min(range(len(held)), key=lambda r: ((held[r] + sizes[s]) / capacities[r], r))
         owner[s] = r
-        left[r] -= sizes[s]
+        held[r] += sizes[s]
     return owner
 
 
