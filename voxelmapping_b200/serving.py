@@ -569,7 +569,7 @@ def merge_summaries(parts):
     requests, offered rates, sessions, budgets and eviction counters add up;
     throughput is all requests over the slowest rank's makespan; percentiles
     are over every rank's latencies ("_latencies"). Per-rank tick statistics
-    stay under "per_rank". A single part comes back unchanged."""
+    stay under "per_rank". A single part comes back as it is, with ranks = 1."""
     if len(parts) == 1:
         return dict(parts[0], ranks=1)
     out = {"ranks": len(parts), "requests": sum(p["requests"] for p in parts),
