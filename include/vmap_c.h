@@ -350,12 +350,14 @@ vmap_status vmap_snapshot_load(vmap_map* map, const void* src, uint64_t bytes, v
  * the library holds until the process exits.
  *  - count > VMAP_EXPORT_STATIC_MAX_BLOCKS is rejected with
  *    VMAP_ERR_INVALID_ARG (text in vmap_last_error); loop over `first`.
- *  - The first call on a device looks up the array's device address; make
- *    that first call before any stream capture begins.
+ *  - The map's device must be the current device (else
+ *    VMAP_ERR_INVALID_ARG); the array's device address is looked up on
+ *    every call.
  *  - All calls share the one array: calls whose work overlaps on the GPU (other
  *    threads, streams or maps at the same time) race. Each call overwrites what
  *    it uses, so nothing needs clearing between calls.
- *  - Synchronous: returns after the host buffers are filled. */
+ *  - Synchronises `stream` (it reads the block count first) and returns
+ *    after the host buffers are filled, so it cannot be captured. */
 #define VMAP_EXPORT_STATIC_MAX_BLOCKS 256
 vmap_status vmap_export_blocks_static(vmap_map* map, uint32_t first, uint32_t count, int32_t* coords, float* tsdf,
                                       float* weight, uint8_t* rgb, uint32_t* n_blocks, void* stream);

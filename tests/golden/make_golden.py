@@ -1,8 +1,9 @@
 """Generate the golden fixtures that pin the oracle to the reference.
 
-The reference (xingruiyang/VoxelMapping) has no tests and cannot be built here
-(it needs Eigen and OpenCV with CUDA), so the only reference data are the
-constants and tables in its sources. This script parses them into JSON:
+The reference (xingruiyang/VoxelMapping) has no tests and ships no data, so
+the only reference data are the constants and tables in its sources (its
+CUDA build, oracle/ref_harness.cu, is the other anchor). This script parses
+them into JSON:
 
   mc_tables.json  - edgeTable[256] and triTable[256][16] (src/triangle_table.h:7-278)
   constants.json  - BLOCK_SIZE, MIN_DEPTH, MAX_DEPTH (include/map_struct.h:6-10),
@@ -12,7 +13,7 @@ constants and tables in its sources. This script parses them into JSON:
                     (src/ray_tracing.cu:7), interpolation band (ray_tracing.cu:366),
                     mesh buffer size (src/vmapping.cpp:6)
 
-Usage: python tests/golden/make_golden.py [reference-root]
+Usage: python tests/golden/make_golden.py <reference-root>
 """
 import json
 import re
@@ -69,4 +70,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference source tree>")
+    main(sys.argv[1])

@@ -114,12 +114,6 @@ def test_required_bytes_matches_the_documented_layout(case):
     assert L.lib().vmap_required_bytes(C.byref(bad), C.byref(got)) == 1  # VMAP_ERR_INVALID_ARG
 
 
-def test_integration_guide_names_every_entry_point():
-    guide = (ROOT / "INTEGRATION.md").read_text()
-    missing = [n for n in declarations() if n not in guide]
-    assert not missing, missing
-
-
 def test_every_entry_point_refuses_null_and_bad_sizes_without_a_device():
     """Misuse is refused on the host with VMAP_ERR_INVALID_ARG (1) before any
     device call: NULL handles and pointers, batch sizes outside 1..256,

@@ -1,0 +1,211 @@
+"""Parity against the reference's own CUDA build: its src/*.cu compiled
+unchanged for sm_100a against project-written Eigen/OpenCV subsets
+(oracle/ref_harness.cu, oracle/ref_shim/), run on the same GPU and the same
+float32 inputs as the library (depth in metres, poses rounded to float32).
+
+Bars (stated here, checked below):
+  * stock reference (single-try bucket locks, include/map_struct.h:331,339),
+    room_small, all 100 frames: every block the reference allocates is one
+    the library allocates (reference set is a subset); the blocks it skipped
+    are counted, not bounded
+  * completed allocation (the reference's allocation kernel repeated on each
+    frame until it adds nothing): allocated block sets equal, and every
+    block's int16 TSDF code, uint8 weight and colour equal, bit for bit,
+    every 25 frames of all 100 (room_small) and on 640x480 frames (room_full)
+  * raycast at the last pose: hit/miss disagreement <= 0.5 % of pixels and
+    >= 99.5 % of common hits within 1 mm (the library skips unallocated
+    blocks in one jump where the reference takes 1-voxel steps)
+  * the reference's computeNormal and Phong kernels on the library's vertex
+    map: normals bit-exact on every pixel the reference writes, Phong within
+    1 of 255
+  * marching cubes: the reference's triangle multiset equals the library's
+    (vertices and face normals bit for bit); surface points bit-exact
+Blocks whose hash bucket is the last one are left out of the comparisons:
+the harness keeps that bucket locked in the reference build (it would
+otherwise be able to point its chain at itself and loop; see
+oracle/ref_harness.cu).
+"""
+import numpy as np
+import pytest
+import torch
+
+from oracle import refbuild as R
+from tests.common import block_keys, raycast_stats, sorted_rows
+from voxelmapping_b200 import VoxelMapping, synth
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not R.available(), reason="reference build missing (make -C oracle ref)")]
+
+SMALL = synth.WORKLOADS["room_small"]
+FULL = synth.WORKLOADS["room_full"]
+
+
+def f32_pose(p):
+    """The reference takes a float Matrix4f: round the pose once and give
+    both builds the same values."""
+    return np.asarray(p, np.float32).astype(np.float64)
+
+
+def product(wl, color, mode=0, fmt="ref"):
+    vm = VoxelMapping(wl.width, wl.height, wl.K, voxel_format=fmt, with_color=color, max_weight=255,
+                      raycast_mode=mode)
+    vm.CreateMap(wl.num_entries, wl.num_blocks, wl.voxel_size)
+    return vm
+
+
+def reference(wl, color):
+    return R.RefMap(wl.width, wl.height, wl.K, wl.num_entries, wl.num_blocks, wl.voxel_size, with_color=color)
+
+
+def fuse_pair(vm, rm, d, rgb, pose, complete):
+    dm = torch.from_numpy(synth.depth_to_metres(d)).cuda()
+    if rgb is not None:
+        c = torch.from_numpy(np.ascontiguousarray(rgb)).cuda()
+        vm.FuseDepthAndImage(c.reshape(rgb.shape[0], -1), dm, pose)
+        return rm.fuse(dm, pose, rgb=c, complete=complete)
+    vm.FuseDepth(dm, pose)
+    return rm.fuse(dm, pose, complete=complete)
+
+
+def last_bucket_mask(coords, n_bucket):
+    return R.hash_bucket(coords, n_bucket) == n_bucket - 1
+
+
+def compare_maps(vm, rm, color, exact=True):
+    """Returns (product-only blocks, reference-only blocks, duplicates)."""
+    info = rm.info()
+    g = vm.export_blocks(with_rgb=color)
+    r = rm.export()
+    keep = ~last_bucket_mask(g["coords"], info["buckets"])
+    gk = block_keys(g["coords"])[keep]
+    rk_all = block_keys(r["coords"])
+    rk, first = np.unique(rk_all, return_index=True)
+    dups = len(rk_all) - len(rk)
+    # duplicates (the reference's racy chain walk) must hold identical voxels
+    if dups:
+        order = np.argsort(rk_all, kind="stable")
+        srt = rk_all[order]
+        same = np.nonzero(srt[1:] == srt[:-1])[0]
+        for i in same:
+            a, b = order[i], order[i + 1]
+            assert np.array_equal(r["codes"][a], r["codes"][b]) and np.array_equal(r["weight"][a], r["weight"][b])
+    only_g = np.setdiff1d(gk, rk)
+    only_r = np.setdiff1d(rk, gk)
+    if exact:
+        assert only_g.size == 0 and only_r.size == 0, (only_g.size, only_r.size)
+        gi = np.argsort(gk)
+        gsel = np.nonzero(keep)[0][gi]
+        ri = first  # sorted by key, like gk[gi]
+        assert np.array_equal(np.sort(gk), rk)
+        tg, tr = g["tsdf"][gsel], r["tsdf"][ri]
+        assert np.array_equal(tg, tr), "tsdf codes differ in %d voxels" % int((tg != tr).sum())
+        assert np.array_equal(g["weight"][gsel], r["weight"][ri])
+        if color:
+            assert np.array_equal(g["rgb"][gsel], r["rgb"][ri])
+    return only_g.size, only_r.size, dups
+
+
+def test_stock_reference_blocks_are_a_subset_room_small():
+    scene = synth.Scene(SMALL)
+    vm, rm = product(SMALL, False), reference(SMALL, False)
+    for i in range(SMALL.n_poses):
+        d, _, pose = scene.render(i)
+        fuse_pair(vm, rm, d, None, f32_pose(pose), complete=False)
+    only_g, only_r, dups = compare_maps(vm, rm, False, exact=False)
+    n = vm.stats()["allocated_blocks"]
+    print("stock reference over 100 frames: product %d blocks, reference skipped %d, reference-only %d, "
+          "duplicate entries %d" % (n, only_g, only_r, dups))
+    assert only_r == 0
+    assert only_g <= 0.05 * n
+
+
+def test_complete_allocation_room_small_all_frames():
+    scene = synth.Scene(SMALL)
+    vm, rm = product(SMALL, False, mode=0), reference(SMALL, False)
+    vm1 = product(SMALL, False, mode=1)
+    for i in range(SMALL.n_poses):
+        d, _, pose = scene.render(i)
+        pose = f32_pose(pose)
+        fuse_pair(vm, rm, d, None, pose, complete=True)
+        dm = torch.from_numpy(synth.depth_to_metres(d)).cuda()
+        vm1.FuseDepth(dm, pose)
+        if i % 25 == 24:
+            compare_maps(vm, rm, False)
+    # raycast at the last pose: the library's tile-bounded march (mode 0) and
+    # its full march (mode 1) against the reference's
+    v_r = rm.render(pose).cpu().numpy()
+    for m in (vm, vm1):
+        nmap = torch.empty((SMALL.height, SMALL.width, 4), dtype=torch.float32, device="cuda")
+        vmap = m.RenderScene(None, pose, nmap=nmap)
+        st = raycast_stats(vmap.cpu().numpy(), v_r)
+        print("raycast vs reference build", st)
+        assert st["mismatch"] <= 0.005 and st["frac_within_1mm"] >= 0.995, st
+    # normals and Phong: the reference's kernels on the library's vertex map
+    n_r = R.compute_normal(vmap).cpu().numpy()
+    n_g = nmap.cpu().numpy()
+    written = ~np.isnan(n_r[..., 3])
+    assert written[:-1, :-1].all() and not written[-1].any() and not written[:, -1].any()
+    xyz_r, xyz_g = n_r[..., :3][written], n_g[..., :3][written]
+    assert np.array_equal(np.isnan(xyz_r), np.isnan(xyz_g))
+    ok = ~np.isnan(xyz_r)
+    assert np.array_equal(xyz_r[ok], xyz_g[ok])
+    from voxelmapping_b200 import _lib as L
+    rgba = torch.empty((SMALL.height, SMALL.width, 4), dtype=torch.uint8, device="cuda")
+    L.check(L.lib().vmap_render_phong(vmap.data_ptr(), 0, nmap.data_ptr(), 0, rgba.data_ptr(), 0, SMALL.width,
+                                      SMALL.height, torch.cuda.current_stream().cuda_stream))
+    p_r = R.render_phong(vmap, nmap).cpu().numpy().astype(int)
+    p_g = rgba.cpu().numpy().astype(int)
+    inner = np.zeros(p_r.shape[:2], bool)
+    inner[:-1, :-1] = True
+    assert np.abs(p_g - p_r)[inner].max() <= 1
+    # marching cubes over the whole map
+    n_g, v_g, nn_g = vm.Polygonize()
+    n_r, v_rr, nn_r, _ = rm.polygonize(n_g + 1024)
+    print("triangles: library %d, reference %d" % (n_g, n_r))
+    info = rm.info()
+    if (last_bucket_mask(vm.export_blocks(with_rgb=False)["coords"], info["buckets"])).any():
+        pytest.skip("a block of the last bucket is missing from the reference build; mesh not comparable")
+    assert n_g == n_r > 10000
+    a = sorted_rows(np.concatenate([v_g, nn_g], axis=1))
+    b = sorted_rows(np.concatenate([v_rr, nn_r], axis=1))
+    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+def test_complete_allocation_with_colour_room_small():
+    scene = synth.Scene(SMALL)
+    vm, rm = product(SMALL, True), reference(SMALL, True)
+    for i in range(0, 40, 2):
+        d, rgb, pose = scene.render(i)
+        fuse_pair(vm, rm, d, rgb, f32_pose(pose), complete=True)
+    compare_maps(vm, rm, True)
+
+
+def test_complete_allocation_room_full_frames():
+    """640x480, 5 mm, 2^21 entries, 2^20 blocks: the full configuration's
+    frames through both builds, colour included."""
+    scene = synth.Scene(FULL)
+    vm, rm = product(FULL, True), reference(FULL, True)
+    for k, i in enumerate(range(0, 120, 6)):
+        d, rgb, pose = scene.render(i)
+        vis, _ = fuse_pair(vm, rm, d, rgb, f32_pose(pose), complete=True)
+        if k % 5 == 4:
+            compare_maps(vm, rm, True)
+    assert vm.stats()["allocated_blocks"] > 15000
+    v_r = rm.render(f32_pose(pose)).cpu().numpy()
+    st = raycast_stats(vm.RenderScene(None, f32_pose(pose)).cpu().numpy(), v_r)
+    print("full-size raycast vs reference build", st)
+    assert st["mismatch"] <= 0.005 and st["frac_within_1mm"] >= 0.995, st
+
+
+def test_surface_points_match_reference():
+    scene = synth.Scene(SMALL)
+    vm, rm = product(SMALL, False), reference(SMALL, False)
+    for i in range(0, 8, 2):
+        d, _, pose = scene.render(i)
+        fuse_pair(vm, rm, d, None, f32_pose(pose), complete=True)
+    n, v, _ = vm.Polygonize()
+    vt = torch.from_numpy(np.ascontiguousarray(v)).cuda()
+    pts = torch.empty((n, 3), dtype=torch.float32, device="cuda")
+    assert R.lib().ref_surface_points(vt.data_ptr(), pts.data_ptr(), n) == 0 and R.lib().ref_sync() == 0
+    g = vm.GetSurfacePoints()
+    assert np.array_equal(sorted_rows(g), sorted_rows(pts.cpu().numpy()))

@@ -46,16 +46,10 @@ def test_cpp_drop_in_program_links(tmp_path):
     assert r.returncode == 0, r.stderr
 
 
-def test_integration_cpp_snippet_compiles(tmp_path):
-    """The C++ example in INTEGRATION.md uses the class as declared: its body,
-    with the caller's buffers and pose as parameters, compiles."""
-    text = (ROOT / "INTEGRATION.md").read_text()
-    block = text.split("```cpp", 1)[1].split("```", 1)[0]
-    body = "\n".join(l for l in block.splitlines() if not l.lstrip().startswith("#include"))
-    src = tmp_path / "snippet.cpp"
-    src.write_text('#include "vmapping.h"\n'
-                   "void snippet(void* depth_dev, const unsigned char* rgb_host, const float* depth_host,\n"
-                   "             const vmap::Mat4f& cam_to_world) {\n" + body + "\n(void)n; (void)points;\n}\n")
+def test_drop_in_example_compiles():
+    """tests/cpp/drop_in_example.cpp, the drop-in use of the class (construct,
+    CreateMap, fuse from device and host buffers, render, mesh), compiles
+    against include/vmapping.h as declared."""
     r = subprocess.run([compiler("g++"), "-std=c++17", "-Wall", "-Werror", "-fsyntax-only", "-I" + str(ROOT / "include"),
-                        str(src)], capture_output=True, text=True)
+                        str(ROOT / "tests" / "cpp" / "drop_in_example.cpp")], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr

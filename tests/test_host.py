@@ -127,3 +127,12 @@ def test_figure8_trajectory_keeps_clear_of_spheres():
     for P in s.poses:
         d = np.linalg.norm(sp[:, :3] - P[:3, 3], axis=1) - sp[:, 3]
         assert d.min() > 0.1
+
+
+def test_static_export_source_allocates_nothing():
+    """The no-allocation export calls no allocating or freeing routine."""
+    src = (Path(__file__).resolve().parent.parent / "voxelmapping_b200" / "csrc" / "export_static.cu").read_text()
+    code = "\n".join(l.split("//")[0] for l in src.splitlines())
+    for name in ("cudaMalloc", "cudaMallocAsync", "cudaMallocHost", "cudaHostAlloc", "cudaMallocManaged", "cudaFree",
+                 "malloc(", "new "):
+        assert name not in code, name

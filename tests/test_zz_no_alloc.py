@@ -66,6 +66,36 @@ def test_static_export_matches_allocating_export_on_two_calls():
     vm.release()
 
 
+@pytest.mark.parametrize("fmt", ["ref", "i16"])
+def test_static_export_without_colour_tsdf_only(fmt):
+    """A map without colour, and only the TSDF requested (the other outputs
+    NULL): the same TSDF as vmap_export_blocks, on two calls in a row."""
+    wl = synth.WORKLOADS["room_small"]
+    scene = synth.Scene(wl)
+    vm = VoxelMapping(wl.width, wl.height, wl.K, voxel_format=fmt, with_color=False)
+    vm.CreateMap(wl.num_entries, wl.num_blocks, wl.voxel_size)
+    for i in (1, 5):
+        d, _, pose = scene.render(i)
+        vm.FuseDepth(torch.from_numpy(d.view(np.int16)).cuda(), pose)
+    ref = vm.export_blocks(with_rgb=False)
+    n = ref["coords"].shape[0]
+    stream = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        tsdf = np.zeros((n, 512), np.float32)
+        for first in range(0, n, MAX_BLOCKS):
+            got = C.c_uint32()
+            L.check(L.lib().vmap_export_blocks_static(vm._map, first, MAX_BLOCKS, None, tsdf[first:].ctypes.data, None,
+                                                      None, C.byref(got), stream), "vmap_export_blocks_static")
+            assert got.value == min(MAX_BLOCKS, n - first)
+        assert np.array_equal(tsdf, ref["tsdf"])
+    # colour requested from a map without colour: refused
+    buf = np.zeros((1, 512, 3), np.uint8)
+    got = C.c_uint32()
+    assert L.lib().vmap_export_blocks_static(vm._map, 0, 1, None, None, None, buf.ctypes.data, C.byref(got),
+                                             stream) == 1
+    vm.release()
+
+
 def test_static_export_rejects_more_than_its_staging_holds():
     wl = synth.WORKLOADS["room_small"]
     vm = VoxelMapping(wl.width, wl.height, wl.K, voxel_format="ref", with_color=False)

@@ -120,9 +120,13 @@ def ptxas_report(sources=("raymarch.cu", "fusion.cu", "mesh.cu", "raycast.cu", "
 
 
 def build_oracle(verbose=False):
-    """Compile the CPU oracle (test infrastructure) with its Makefile."""
-    _run(["make", "-s", "-C", ROOT / "oracle", "CC=" + ("/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc")],
-         verbose)
+    """Compile the checkers (test infrastructure) with oracle/Makefile: the
+    CPU oracle, and the reference's own CUDA build (oracle/_ref/) when the
+    reference sources are present; where they are not, a prebuilt
+    oracle/_ref/ is used as it is."""
+    cc = "CC=" + ("/usr/bin/gcc" if Path("/usr/bin/gcc").exists() else "gcc")
+    _run(["make", "-s", "-C", ROOT / "oracle", cc], verbose)
+    _run(["make", "-s", "-C", ROOT / "oracle", cc, "NVCC=" + nvcc(), "ref-if-present"], verbose)
     return ROOT / "oracle" / "libvmap_oracle.so"
 
 

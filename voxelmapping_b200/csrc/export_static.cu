@@ -11,8 +11,9 @@
 // The array is a file-scope __device__ variable: every GPU that loads the
 // library holds it (about 1.4 MiB) until the process exits. In host code its
 // name is only a host-side stand-in, so its device address is looked up with
-// cudaGetSymbolAddress, once per device, on that device's first call.
-#include <mutex>
+// cudaGetSymbolAddress on every call, on the map's device (a lookup: it
+// allocates nothing, and it stays right if the application tears its context
+// down and the module is loaded again at another address).
 #include <string>
 
 #include "vmap_launch.h"
@@ -31,30 +32,14 @@ constexpr size_t kStageBytes = kMaxBlocks * (kStageCoords + kStageTsdf + kStageW
 
 static __device__ __align__(256) unsigned char g_export_stage[kStageBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_stage_mutex;
-unsigned char* g_stage_addr[kMaxDevices];  // device address of g_export_stage, per device
-
-// Device address of the staging array on the current device (looked up on the
-// first call per device; that call must not be inside a stream capture).
+// Device address of the staging array on the current device.
 cudaError_t stage_address(unsigned char** out)
 {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess) return e;
-    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    std::lock_guard<std::mutex> lock(g_stage_mutex);
-    if (!g_stage_addr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_export_stage);
-        if (e != cudaSuccess) return e;
-        g_stage_addr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = g_stage_addr[dev];
-    return cudaSuccess;
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_export_stage);
+    if (e == cudaSuccess) *out = static_cast<unsigned char*>(p);
+    return e;
 }
-
-
 
 }  // namespace
 
@@ -72,6 +57,13 @@ extern "C" vmap_status vmap_export_blocks_static(vmap_map* map, uint32_t first, 
     vmap_status st = vmap_get_config(map, &cfg);
     if (st != VMAP_OK) return st;
     if (rgb && !cfg.with_color) return VMAP_ERR_INVALID_ARG;
+    // the staging array used is the current device's: it must be the map's
+    int cur = -1;
+    if (cudaGetDevice(&cur) != cudaSuccess || cur != map_device(map)) {
+        set_last_error("vmap_export_blocks_static: the current device (" + std::to_string(cur) +
+                       ") is not the map's device (" + std::to_string(map_device(map)) + ")");
+        return VMAP_ERR_INVALID_ARG;
+    }
     vmap_stats s;
     if ((st = vmap_get_stats(map, stream, &s)) != VMAP_OK) return st;  // synchronises `stream`
     const uint32_t n = first >= s.allocated_blocks ? 0u

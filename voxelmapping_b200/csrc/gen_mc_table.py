@@ -90,4 +90,6 @@ def main(src):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/triangle_table.h")
+    if len(sys.argv) != 2:
+        sys.exit("usage: gen_mc_table.py <reference tree>/src/triangle_table.h")
+    main(sys.argv[1])

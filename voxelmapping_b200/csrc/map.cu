@@ -936,5 +936,6 @@ vmap_status vmap_export_blocks(vmap_map* m, int32_t* coords, float* tsdf, float*
 // Internal accessors for other translation units of the library.
 namespace vmapb {
 const DevMap& map_device_view(const vmap_map* m) { return m->dm; }
+int map_device(const vmap_map* m) { return m->device; }
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 }  // namespace vmapb

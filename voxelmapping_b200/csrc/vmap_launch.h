@@ -98,6 +98,7 @@ cudaError_t launch_export(const DevMap& m, int fmt, bool color, int first, int c
 
 // map.cu: device view of a map and the text behind vmap_last_error().
 const DevMap& map_device_view(const vmap_map* m);
+int map_device(const vmap_map* m);  // CUDA device the map was created on
 void set_last_error(const std::string& msg);
 
 // 32x8-pixel tiles of a W x H image (alloc and normal-map work items)

@@ -632,10 +632,12 @@ def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, 
     if world > 1:
         free, _ = torch.cuda.mem_get_info()
         owner = partition_sessions([session_bytes(w) for w in all_wls], all_gather(free))
+    # the partition is the same on every rank: every rank refuses it together
+    empty = sorted(set(range(world)) - set(owner))
+    if empty:
+        raise ValueError("rank(s) %s hold no session (%d sessions over %d ranks)" % (empty, total, world))
     wls = [all_wls[s] for s in range(total) if owner[s] == rank]
     n_local = len(wls)
-    if n_local == 0:
-        raise ValueError("rank %d holds no session" % rank)
     frames = render_frames(wls, n_frames)
     ex = GpuExecutor(wls, frames, keep_results=keep_results)
     sizes = [ex.session_bytes(s) for s in range(n_local)]
@@ -667,7 +669,15 @@ def run_serving(n_sessions=256, rates=(2000.0,), count=4000, budget_bytes=None, 
             reqs, stats = serve(reqs, sched, ex)
             summ = summarize(reqs, stats)
             summ["phase_s"] = {k: round(v, 4) for k, v in ex.phase.items()}
-            summ.update({"offered_rps": rate * world * n_local / total, "sessions": n_local, "budget_gb": budget / 1e9,
+            # offered_rps: this rank's share of the job's Poisson rate by
+            # session count (requests pick sessions uniformly, so it is the
+            # expected rate; summed over ranks it is the job's rate);
+            # offered_rps_measured: its requests over the span of their
+            # arrival times, the rate this rank actually drew
+            span = (max(r.arrival for r in reqs) - min(r.arrival for r in reqs)) if len(reqs) > 1 else 0.0
+            summ.update({"offered_rps": rate * world * n_local / total,
+                         "offered_rps_measured": (len(reqs) - 1) / span if span > 0 else None,
+                         "sessions": n_local, "budget_gb": budget / 1e9,
                          "all_sessions_gb": sum(sizes) / 1e9})
             results.append(summ)
             if log:
