@@ -52,6 +52,9 @@ def lib():
             "orc_polygonize": (C.c_long, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_long]),
             "orc_surface_points": (None, [C.c_void_p, C.c_long, C.c_void_p]),
             "orc_num_blocks": (C.c_int, [C.c_void_p]),
+            "orc_last_raycast_blocks": (C.c_int, [C.c_void_p]),
+            "orc_last_alloc_blocks": (C.c_int, [C.c_void_p]),
+            "orc_probe": (None, [C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
             "orc_export": (None, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]),
             "orc_hash": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int]),
             "orc_pose_inverse": (None, [D16, D16]),
@@ -126,6 +129,14 @@ class OracleMap:
     def num_blocks(self):
         return lib().orc_num_blocks(self._h)
 
+    def last_alloc_blocks(self):
+        """Unique blocks the last fused frame's allocation touched (its A)."""
+        return lib().orc_last_alloc_blocks(self._h)
+
+    def last_raycast_blocks(self):
+        """Unique allocated blocks the last raycast read (its U)."""
+        return lib().orc_last_raycast_blocks(self._h)
+
     def export(self):
         n = self.num_blocks()
         coords = np.zeros((n, 3), np.int32)
@@ -166,6 +177,17 @@ def surface_points(verts):
     v = np.ascontiguousarray(verts, np.float32)
     out = np.empty((v.shape[0], 3), np.float32)
     lib().orc_surface_points(_ptr(v), v.shape[0], _ptr(out))
+    return out
+
+
+def probe(which, inputs):
+    """The reference build's arithmetic probe shape `which` (an index of
+    oracle.refbuild.PROBES) on each row of `inputs` (n, <=20) float32,
+    through the oracle's FP32 helpers; returns (n, 4) float32."""
+    x = np.zeros((len(inputs), 20), np.float32)
+    x[:, :inputs.shape[1]] = inputs
+    out = np.empty((len(inputs), 4), np.float32)
+    lib().orc_probe(int(which), _ptr(x), len(inputs), _ptr(out))
     return out
 
 

@@ -17,13 +17,14 @@ static void FN(make_xform)(const double p[16], FN(xform_t) * t)
         for (int c = 0; c < 4; ++c) t->m[r][c] = (R)p[4 * r + c];
 }
 
-/* Eigen Transform<.,3,Affine> * Vector3 (map_struct.h:201,212): translation +
- * lazy coefficient product, whose redux sums c0 + (c1 + c2); nvcc contracts
- * each product into the following add. */
+/* Eigen 3.3 Transform<.,3,Affine> * Vector3 (map_struct.h:201,212): the 4x4
+ * matrix times (v, 1), each row's redux in halves, (c0 + c1) + (c2 + c3) with
+ * c3 = m_i3 * 1; nvcc contracts the first product of each half. Pinned by the
+ * arithmetic probe of the reference's own build (oracle/ref_harness.cu). */
 static inline void FN(xform_pt)(const FN(xform_t) * t, const R v[3], R out[3])
 {
     for (int i = 0; i < 3; ++i)
-        out[i] = t->m[i][3] + FMA(t->m[i][0], v[0], FMA(t->m[i][1], v[1], t->m[i][2] * v[2]));
+        out[i] = FMA(t->m[i][0], v[0], t->m[i][1] * v[1]) + FMA(t->m[i][2], v[2], t->m[i][3]);
 }
 
 /* unproject (map_struct.h:189-194): (ifx*(x-cx))*z, (ify*(y-cy))*z, z */
@@ -37,10 +38,12 @@ static inline void FN(unproject)(int x, int y, R z, R ifx, R ify, R cx, R cy, R 
 /* Eigen squaredNorm(): v0^2 + (v1^2 + v2^2) with contraction. */
 static inline R FN(sqnorm)(const R v[3]) { return FMA(v[0], v[0], FMA(v[1], v[1], v[2] * v[2])); }
 
-/* Eigen normalized(): v / sqrt(|v|^2) when |v|^2 > 0, else v unchanged. */
+/* Eigen normalized(): v / sqrt(|v|^2) when |v|^2 > 0, else v unchanged.
+ * Inside normalized() nvcc contracts the squared norm as v0^2 + (v2^2 + v1^2)
+ * (pinned by the arithmetic probe of the reference's own build). */
 static inline void FN(normalize)(R v[3])
 {
-    R s = FN(sqnorm)(v);
+    R s = FMA(v[0], v[0], FMA(v[2], v[2], v[1] * v[1]));
     if (s > 0) {
         R n = SQRT(s);
         v[0] = v[0] / n;
@@ -195,9 +198,23 @@ static int FN(allocate)(orc_map* m, const float* depth, const double pose[16], i
             if (r == 1) n_new++;
             else if (r < 0) n_failed++;
         }
+    }
+    /* unique blocks the frame's band samples touched (its A) */
+    uint8_t* seen = (uint8_t*)calloc(m->nblk > 0 ? (size_t)m->nblk : 1, 1);
+    int touched = 0;
+    for (int y = 0; y < H; ++y) {
+        for (int k = 0; k < rows[y].n; ++k) {
+            const int bi = orc_find(m, rows[y].b + 3 * (size_t)k);
+            if (bi >= 0 && !seen[bi]) {
+                seen[bi] = 1;
+                touched++;
+            }
+        }
         free(rows[y].b);
     }
+    free(seen);
     free(rows);
+    m->last_alloc_blocks = touched;
     if (n_failed_out) *n_failed_out = n_failed;
     return n_new;
 }
@@ -265,7 +282,9 @@ static int FN(integrate)(orc_map* m, const float* depth, const uint8_t* rgb, con
 }
 
 /* ---- raycast: MapRenderingDelegate (ray_tracing.cu:272-400) --------------- */
-typedef struct { int32_t key[3]; int32_t blk; } FN(cache_t);
+/* lookup cache of one ray (or cube); `touched`, when set, marks every
+ * allocated block a lookup finds (the unique blocks any ray sampled) */
+typedef struct { int32_t key[3]; int32_t blk; uint8_t* touched; } FN(cache_t);
 
 static inline R FN(read_sdf)(const orc_map* m, FN(cache_t) * cache, const R p[3], int* valid)
 {
@@ -277,6 +296,7 @@ static inline R FN(read_sdf)(const orc_map* m, FN(cache_t) * cache, const R p[3]
     if (b[0] != cache->key[0] || b[1] != cache->key[1] || b[2] != cache->key[2]) {
         memcpy(cache->key, b, 12);
         cache->blk = orc_find(m, b);
+        if (cache->touched && cache->blk >= 0) cache->touched[cache->blk] = 1;
     }
     if (cache->blk >= 0) {
         const size_t vi = (size_t)cache->blk * 512 + (size_t)voxel_local_idx(v);
@@ -310,7 +330,7 @@ static R FN(read_sdf_interp)(const orc_map* m, FN(cache_t) * cache, const R p[3]
     return FMA((R)1 - fz, r2, fz * r3);
 }
 
-static int FN(raycast)(const orc_map* m, const double pose[16], float* vmap)
+static int FN(raycast)(const orc_map* m, const double pose[16], float* vmap, uint8_t* touched)
 {
     const orc_config* c = &m->cfg;
     const int W = c->width, H = c->height;
@@ -326,7 +346,7 @@ static int FN(raycast)(const orc_map* m, const double pose[16], float* vmap)
     int hits = 0;
 #pragma omp parallel for schedule(dynamic, 2) reduction(+ : hits)
     for (int y = 0; y < H; ++y) {
-        FN(cache_t) cache = {{INT32_MIN, INT32_MIN, INT32_MIN}, -1};
+        FN(cache_t) cache = {{INT32_MIN, INT32_MIN, INT32_MIN}, -1, touched};
         for (int x = 0; x < W; ++x) {
             float* out = vmap + 4 * ((size_t)y * W + x);
             out[0] = out[1] = out[2] = out[3] = NAN;
@@ -431,7 +451,7 @@ static long FN(polygonize)(const orc_map* m, float* verts, float* norms, long ma
     long* cnt = (long*)calloc((size_t)nb + 1, sizeof(long));
 #pragma omp parallel for schedule(dynamic, 16)
     for (int b = 0; b < nb; ++b) {
-        FN(cache_t) cache = {{INT32_MIN, INT32_MIN, INT32_MIN}, -1};
+        FN(cache_t) cache = {{INT32_MIN, INT32_MIN, INT32_MIN}, -1, NULL};
         R vv[12][3];
         long n = 0;
         const int32_t* bp = m->coords + 3 * (size_t)b;
@@ -450,7 +470,7 @@ static long FN(polygonize)(const orc_map* m, float* verts, float* norms, long ma
 #pragma omp parallel for schedule(dynamic, 16)
         for (int b = 0; b < nb; ++b) {
             if (cnt[b] >= max_tris) continue;
-            FN(cache_t) cache = {{INT32_MIN, INT32_MIN, INT32_MIN}, -1};
+            FN(cache_t) cache = {{INT32_MIN, INT32_MIN, INT32_MIN}, -1, NULL};
             R vv[12][3];
             long t = cnt[b];
             const int32_t* bp = m->coords + 3 * (size_t)b;

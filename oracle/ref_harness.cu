@@ -165,6 +165,99 @@ int render(RefMap* r, vmap::MapStruct<TVoxel>& m, float* vmap_dev, std::size_t p
     return int(r->numVisBlock);
 }
 
+
+// Arithmetic probe: each floating-point expression shape of the reference,
+// evaluated on caller inputs by the reference's own device functions (or its
+// literal expression, compiled in this same translation unit with the same
+// flags, through the Eigen subset). Shows which multiply nvcc fuses into
+// which add, expression by expression. Inputs: 20 floats per item; outputs:
+// 4 floats per item.
+__global__ void probe_kernel(int which, const float* in, int n, float* out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float* a = in + (size_t)i * 20;
+    float* o = out + (size_t)i * 4;
+    Eigen::Matrix4f M;
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 4; ++c) M(r, c) = a[4 * r + c];
+    M(3, 0) = M(3, 1) = M(3, 2) = 0.f;
+    M(3, 3) = 1.f;
+    switch (which) {
+    case 0: {  // Transform<float,3,Affine> * Vector3f
+        Eigen::Transform<float, 3, Eigen::Affine> T;
+        T = M;
+        Eigen::Vector3f r = T * Eigen::Vector3f(a[12], a[13], a[14]);
+        o[0] = r(0), o[1] = r(1), o[2] = r(2);
+        break;
+    }
+    case 1: {  // unprojectWorld (map_struct.h:196-202)
+        Eigen::Transform<float, 3, Eigen::Affine> T;
+        T = M;
+        Eigen::Vector3f r = vmap::unprojectWorld(int(a[12]), int(a[13]), a[14], a[15], a[16], a[17], a[18], T);
+        o[0] = r(0), o[1] = r(1), o[2] = r(2);
+        break;
+    }
+    case 2: {  // project (map_struct.h:182-187)
+        Eigen::Vector2f r = vmap::project(Eigen::Vector3f(a[0], a[1], a[2]), a[3], a[4], a[5], a[6]);
+        o[0] = r(0), o[1] = r(1);
+        break;
+    }
+    case 3: o[0] = Eigen::Vector3f(a[0], a[1], a[2]).squaredNorm(); break;
+    case 4: o[0] = Eigen::Vector3f(a[0], a[1], a[2]).norm(); break;
+    case 5: {
+        Eigen::Vector3f r = Eigen::Vector3f(a[0], a[1], a[2]).normalized();
+        o[0] = r(0), o[1] = r(1), o[2] = r(2);
+        break;
+    }
+    case 6: {
+        Eigen::Vector3f r = Eigen::Vector3f(a[0], a[1], a[2]).cross(Eigen::Vector3f(a[3], a[4], a[5]));
+        o[0] = r(0), o[1] = r(1), o[2] = r(2);
+        break;
+    }
+    case 7: o[0] = Eigen::Vector3f(a[0], a[1], a[2]).dot(Eigen::Vector3f(a[3], a[4], a[5])); break;
+    case 8: {  // one lerp of read_sdf_interped (ray_tracing.cu:300)
+        float x = a[0], s0 = a[1], s1 = a[2];
+        o[0] = (1.0f - x) * s0 + x * s1;
+        break;
+    }
+    case 9: {  // running average (depth_fusion.cu:190)
+        float oldSDF = a[0], sdf = a[2];
+        unsigned char oldWT = (unsigned char)a[1];
+        o[0] = (oldSDF * oldWT + sdf * 1) / (oldWT + 1);
+        break;
+    }
+    case 10: {  // colour blend (depth_fusion.cu:377)
+        Vector3b oldRGB((unsigned char)a[0], (unsigned char)a[1], (unsigned char)a[2]);
+        Eigen::Vector3f RGB(a[3], a[4], a[5]);
+        Vector3b r = (0.7f * oldRGB.cast<float>() + 0.3f * RGB).cast<unsigned char>();
+        o[0] = r(0), o[1] = r(1), o[2] = r(2);
+        break;
+    }
+    case 11: {  // ray step (ray_tracing.cu:376)
+        Eigen::Vector3f result(a[0], a[1], a[2]), dir(a[4], a[5], a[6]);
+        float step = a[3];
+        result += step * dir;
+        o[0] = result(0), o[1] = result(1), o[2] = result(2);
+        break;
+    }
+    case 12: {  // renderPoint (image_proc.cu:8-44)
+        Eigen::Matrix<uchar, 4, 1> r = vmap::renderPoint(Eigen::Vector3f(a[0], a[1], a[2]),
+                                                         Eigen::Vector3f(a[3], a[4], a[5]), Eigen::Vector3f(1.f, 1.f, 1.f),
+                                                         Eigen::Vector3f(a[6], a[7], a[8]));
+        o[0] = r(0), o[1] = r(1), o[2] = r(2), o[3] = r(3);
+        break;
+    }
+    case 13: {  // interpolateLinear (marching_cubes.cu:106-115)
+        vmap::BuildVertexArray<vmap::Voxel> b;
+        float v1 = a[0], v2 = a[1];
+        o[0] = b.interpolateLinear(v1, v2);
+        break;
+    }
+    default: break;
+    }
+}
+
 } // namespace
 
 extern "C" {
@@ -359,6 +452,16 @@ int ref_copy_map(void* h, void* hash_host, void* pool_host, int blocks)
         REF_TRY(cudaMemcpy(pool_host, r->plain.voxelBlock, sizeof(vmap::Voxel) * BLOCK_SIZE_3 * std::size_t(blocks),
                            cudaMemcpyDeviceToHost));
     }
+    return 0;
+}
+
+/* Arithmetic probe (see probe_kernel): in = 20 floats per item (device),
+ * out = 4 floats per item (device). */
+int ref_probe(int which, const float* in_dev, int n, float* out_dev)
+{
+    if (n <= 0) return 0;
+    probe_kernel<<<(n + 127) / 128, 128>>>(which, in_dev, n, out_dev);
+    REF_TRY(cudaDeviceSynchronize());
     return 0;
 }
 

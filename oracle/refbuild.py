@@ -35,6 +35,7 @@ SYMBOLS = {
     "ref_surface_points": (C.c_int, [C.c_void_p, C.c_void_p, C.c_uint]),
     "ref_info": (C.c_int, [C.c_void_p, C.POINTER(C.c_int)]),
     "ref_copy_map": (C.c_int, [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int]),
+    "ref_probe": (C.c_int, [C.c_int, C.c_void_p, C.c_int, C.c_void_p]),
     "ref_sync": (C.c_int, []),
 }
 
@@ -192,3 +193,20 @@ def render_phong(vmap, nmap):
            "ref_render_phong")
     _check(lib().ref_sync(), "ref_sync")
     return img
+
+
+PROBES = {"xform": 0, "unproject_world": 1, "project": 2, "squared_norm": 3, "norm": 4, "normalized": 5,
+          "cross": 6, "dot": 7, "lerp": 8, "running_average": 9, "rgb_blend": 10, "ray_step": 11, "phong": 12,
+          "mc_interp": 13}
+
+
+def probe(name, inputs):
+    """Evaluate one of the reference's expression shapes (PROBES) on the GPU
+    for each row of `inputs` (n, <=20) float32; returns (n, 4) float32."""
+    import torch
+    x = np.zeros((len(inputs), 20), np.float32)
+    x[:, :inputs.shape[1]] = inputs
+    xi = torch.from_numpy(x).cuda()
+    out = torch.full((len(inputs), 4), float("nan"), dtype=torch.float32, device="cuda")
+    _check(lib().ref_probe(PROBES[name], xi.data_ptr(), len(inputs), out.data_ptr()), "ref_probe")
+    return out.cpu().numpy()

@@ -36,6 +36,8 @@ struct orc_map {
     int32_t* hkeys;      /* 3 per slot */
     int32_t* hvals;      /* block index or -1 */
     size_t hcap, hcount;
+    int last_raycast_blocks; /* unique allocated blocks the last raycast read */
+    int last_alloc_blocks;   /* unique blocks the last frame's allocation touched */
 };
 
 /* ---- GPU-semantics conversions (cvt.rzi / cvt.rmi saturate, NaN -> 0) ---- */
@@ -284,6 +286,9 @@ void orc_reset(orc_map* m)
     m->cfg = c;
 }
 
+int orc_last_raycast_blocks(const orc_map* m) { return m->last_raycast_blocks; }
+int orc_last_alloc_blocks(const orc_map* m) { return m->last_alloc_blocks; }
+
 void orc_destroy(orc_map* m)
 {
     if (!m) return;
@@ -325,7 +330,13 @@ int orc_fuse(orc_map* m, const float* depth, const uint8_t* rgb, const double po
 
 int orc_raycast(orc_map* m, const double pose[16], float* vmap)
 {
-    return m->cfg.precision == ORC_FP64 ? raycast_d(m, pose, vmap) : raycast_f(m, pose, vmap);
+    uint8_t* touched = (uint8_t*)calloc(m->nblk > 0 ? (size_t)m->nblk : 1, 1);
+    const int hits = m->cfg.precision == ORC_FP64 ? raycast_d(m, pose, vmap, touched) : raycast_f(m, pose, vmap, touched);
+    int u = 0;
+    for (int b = 0; b < m->nblk; ++b) u += touched[b];
+    free(touched);
+    m->last_raycast_blocks = u;
+    return hits;
 }
 
 long orc_polygonize(orc_map* m, float* verts, float* norms, long max_tris)
@@ -438,3 +449,59 @@ void orc_constants(int out[9])
     out[7] = ORC_HASH_P2;
     out[8] = 8;
 }
+
+/* The expression shapes of the reference's arithmetic probe
+ * (oracle/ref_harness.cu, probe_kernel), evaluated with this oracle's FP32
+ * helpers; a GPU test requires both to agree bit for bit. in: 20 floats per
+ * item, out: 4 floats per item (unused lanes NaN). */
+void orc_probe(int which, const float* in, int n, float* out)
+{
+    for (int k = 0; k < n; ++k) {
+        const float* a = in + 20 * (size_t)k;
+        float* o = out + 4 * (size_t)k;
+        o[0] = o[1] = o[2] = o[3] = NAN;
+        xform_t_f T;
+        for (int r = 0; r < 3; ++r)
+            for (int c = 0; c < 4; ++c) T.m[r][c] = a[4 * r + c];
+        switch (which) {
+        case 0: xform_pt_f(&T, a + 12, o); break;
+        case 1: {
+            float u[3];
+            unproject_f((int)a[12], (int)a[13], a[14], a[15], a[16], a[17], a[18], u);
+            xform_pt_f(&T, u, o);
+            break;
+        }
+        case 2:
+            o[0] = a[3] * a[0] / a[2] + a[5];
+            o[1] = a[4] * a[1] / a[2] + a[6];
+            break;
+        case 3: o[0] = sqnorm_f(a); break;
+        case 4: o[0] = sqrtf(sqnorm_f(a)); break;
+        case 5: o[0] = a[0], o[1] = a[1], o[2] = a[2]; normalize_f(o); break;
+        case 6: cross_f(a, a + 3, o); break;
+        case 7: o[0] = fmaf(a[0], a[3], fmaf(a[1], a[4], a[2] * a[5])); break;
+        case 8: o[0] = fmaf(1.0f - a[0], a[1], a[0] * a[2]); break;
+        case 9: {
+            const float w = (float)(unsigned char)a[1];
+            o[0] = fmaf(a[0], w, a[2]) / (w + 1.0f);
+            break;
+        }
+        case 10:
+            for (int i = 0; i < 3; ++i) o[i] = (float)(uint8_t)f2i_rz((double)fmaf(0.7f, a[i], 0.3f * a[3 + i]));
+            break;
+        case 11:
+            for (int i = 0; i < 3; ++i) o[i] = fmaf(a[3], a[4 + i], a[i]);
+            break;
+        case 12: {
+            float p[4] = {a[0], a[1], a[2], 1.f}, nn[4] = {a[3], a[4], a[5], 1.f};
+            uint8_t px[4];
+            orc_render_phong(p, nn, 1, 1, px);
+            for (int i = 0; i < 4; ++i) o[i] = (float)px[i];
+            break;
+        }
+        case 13: o[0] = mc_interp_f(a[0], a[1]); break;
+        default: break;
+        }
+    }
+}
+

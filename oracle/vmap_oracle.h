@@ -84,6 +84,18 @@ int orc_allocate(orc_map* m, const float* depth, const double pose[16], int* n_f
  * miss). Returns the number of hits. */
 int orc_raycast(orc_map* m, const double pose[16], float* vmap);
 
+/* Unique allocated blocks the last orc_raycast read (U of the raycast's
+ * algorithmic bytes: U x 512 voxels are all the voxel data rays can touch). */
+int orc_last_raycast_blocks(const orc_map* m);
+
+/* Unique allocated blocks the last fused frame's allocation samples touched
+ * (A of the fused frame's algorithmic bytes). */
+int orc_last_alloc_blocks(const orc_map* m);
+
+/* The reference build's arithmetic probe shapes (oracle/ref_harness.cu)
+ * through this oracle's FP32 helpers: in 20 floats, out 4 floats per item. */
+void orc_probe(int which, const float* in, int n, float* out);
+
 /* Reference computeNormal on a width*height float4 vertex map. Pixels in the
  * last row/column, or with a NaN neighbour, come out NaN. */
 void orc_compute_normal(const float* vmap, int width, int height, float* nmap);

@@ -72,31 +72,3 @@ def sorted_rows(a):
     a = np.ascontiguousarray(a)
     v = a.view(np.dtype((np.void, a.dtype.itemsize * a.shape[1]))).ravel()
     return a[np.argsort(v, kind="stable")]
-
-
-def frustum_pixels(coords, voxel_size, pose, K, w, h):
-    """Pixels whose rays can cross one of the given blocks: each block's 8
-    corners projected at the pose, bounding box grown by one pixel."""
-    mask = np.zeros((h, w), bool)
-    if len(coords) == 0:
-        return mask
-    inv = np.linalg.inv(pose)
-    s = 8 * voxel_size
-    corners = np.array([[i & 1, (i >> 1) & 1, (i >> 2) & 1] for i in range(8)], np.float64)
-    for c in coords.astype(np.float64):
-        p = (c[None, :] + corners) * s
-        q = p @ inv[:3, :3].T + inv[:3, 3]
-        z = q[:, 2]
-        if (z <= 1e-3).any():  # behind or at the camera: be conservative
-            if (z > 1e-3).any():
-                mask[:] = True
-                return mask
-            continue
-        u = K[0, 0] * q[:, 0] / z + K[0, 2]
-        v = K[1, 1] * q[:, 1] / z + K[1, 2]
-        x0, x1 = int(np.floor(u.min())) - 1, int(np.ceil(u.max())) + 1
-        y0, y1 = int(np.floor(v.min())) - 1, int(np.ceil(v.max())) + 1
-        if x1 < 0 or y1 < 0 or x0 >= w or y0 >= h:
-            continue
-        mask[max(y0, 0):min(y1, h - 1) + 1, max(x0, 0):min(x1, w - 1) + 1] = True
-    return mask

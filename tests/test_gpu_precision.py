@@ -21,7 +21,7 @@ import pytest
 import torch
 
 from oracle import oracle as O
-from tests.common import aligned_maps, block_keys, frustum_pixels, raycast_stats
+from tests.common import aligned_maps, block_keys, raycast_stats
 from voxelmapping_b200 import VoxelMapping
 from voxelmapping_b200 import _lib as L
 from voxelmapping_b200 import synth
@@ -55,6 +55,15 @@ def sweep():
             o.fuse(synth.depth_to_metres(d), None, p)
         n, verts, _ = o.polygonize()
         ref64[cap] = (o, o.raycast(pose), verts)
+    # the reference arithmetic itself (FP32 oracle, FP32 storage) against FP64:
+    # how many pixels the algorithm in single precision puts beyond 1 mm
+    o32 = O.OracleMap(WL.width, WL.height, WL.K, WL.num_blocks, WL.voxel_size, storage="f32", max_weight=128)
+    for d, _, p in frames:
+        o32.fuse(synth.depth_to_metres(d), None, p)
+    v32 = o32.raycast(pose)
+    both32 = np.isfinite(v32[..., 0]) & np.isfinite(ref64[128][1][..., 0])
+    dz32 = np.abs(v32[..., 2] - ref64[128][1][..., 2])[both32]
+    oracle32 = {"over_1mm": int((dz32 > 1e-3).sum()), "max_mm": float(dz32.max() * 1e3)}
     lib = L.lib()
     rows = {}
     f32_map = None  # FP32-storage export: the others minus it isolate storage quantisation
@@ -93,15 +102,8 @@ def sweep():
         q = g["tsdf"][qw].astype(np.float64) - f32_map["tsdf"][qw]
         v = vm.RenderScene(None, pose).cpu().numpy()
         ray = raycast_stats(v, v64)
-        # blocks only one of FP32 / FP64 allocates (a band sample rounding
-        # into a neighbour block) and the pixels whose rays can cross them
-        differ = np.setxor1d(block_keys(g["coords"]), block_keys(r["coords"]))
-        dcoords = np.concatenate([g["coords"][np.isin(block_keys(g["coords"]), differ)],
-                                  r["coords"][np.isin(block_keys(r["coords"]), differ)]])
-        near = frustum_pixels(dcoords, WL.voxel_size, pose, WL.K, WL.width, WL.height)
         hit2 = np.isfinite(v[..., 0]) & np.isfinite(v64[..., 0])
-        clean = hit2 & ~near
-        dz_clean = float(np.abs(v[..., 2] - v64[..., 2])[clean].max() * 1e3) if clean.any() else 0.0
+        over = int((np.abs(v[..., 2] - v64[..., 2])[hit2] > 1e-3).sum())
         k, verts, _ = vm.Polygonize()
         h_max, h_p99 = hausdorff_mm(verts, verts64)
         rows[fmt] = {"weight_cap": cap, "bytes_per_voxel": bpv, "blocks": int(len(g["coords"])),
@@ -113,8 +115,8 @@ def sweep():
                      "weight_mismatch": float((gw != rw).mean()),
                      "raycast_dz_max_mm": ray["dz_max_mm"], "raycast_dz_mean_mm": ray["dz_mean_mm"],
                      "raycast_dz_p999_mm": ray["dz_p999_mm"], "raycast_within_1mm": ray["frac_within_1mm"],
-                     "raycast_dz_max_clean_mm": dz_clean, "raycast_clean_pixels": int(clean.sum()),
-                     "raycast_hit_pixels": int(hit2.sum()),
+                     "raycast_over_1mm": over, "raycast_hit_pixels": int(hit2.sum()),
+                     "oracle_fp32_over_1mm": oracle32["over_1mm"], "oracle_fp32_dz_max_mm": oracle32["max_mm"],
                      "raycast_hit_mismatch": ray["mismatch"], "triangles": int(k),
                      "mesh_hausdorff_mm": h_max, "mesh_hausdorff_p99_mm": h_p99,
                      "fuse_us": fuse_us, "fuse_gbs": float(fuse_bytes / (fuse_us * 1e-6) / 1e9)}
@@ -132,12 +134,16 @@ def sweep():
 
 @pytest.mark.parametrize("fmt", [f for f, _ in FORMATS])
 def test_raycast_depth_within_1mm_of_fp64(sweep, fmt):
-    # every pixel whose rays cannot cross a block that only one of FP32 / FP64
-    # allocates is within 1 mm of the FP64 depth; over all pixels >= 99 %
+    # Depth within 1 mm of FP64 at the 99.9th percentile, with no more pixels
+    # beyond 1 mm than the reference arithmetic itself (the FP32 oracle) puts
+    # there (+ 0.02 % of the hits): the reference's two fixed refinement
+    # steps after the zero crossing (ray_tracing.cu:381-393) do not converge
+    # at oblique incidence, so single precision and double precision can stop
+    # on neighbouring samples and end millimetres apart on a few pixels.
     r = sweep[fmt]
-    assert r["raycast_within_1mm"] >= 0.99 and r["raycast_dz_mean_mm"] <= 0.2, r
-    assert r["raycast_hit_mismatch"] <= 0.01, r
-    assert r["raycast_dz_max_clean_mm"] <= 1.0 and r["raycast_clean_pixels"] > 0.5 * r["raycast_hit_pixels"], r
+    assert r["raycast_within_1mm"] >= 0.999 and r["raycast_dz_p999_mm"] <= 1.0, r
+    assert r["raycast_dz_mean_mm"] <= 0.2 and r["raycast_hit_mismatch"] <= 0.01, r
+    assert r["raycast_over_1mm"] <= 2 * r["oracle_fp32_over_1mm"] + 2e-4 * r["raycast_hit_pixels"], r
 
 
 def test_tsdf_error_ordered_by_storage_precision(sweep):

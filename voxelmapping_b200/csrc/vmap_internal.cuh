@@ -64,14 +64,16 @@ struct DevMap {
 };
 
 // ---------------------------------------------------------------- FP32 math
-// Transform<float,3,Affine> * Vector3f (map_struct.h:201,212):
-// t_i + (m_i0 v0 + (m_i1 v1 + m_i2 v2)), each product contracted into its add.
+// Transform<float,3,Affine> * Vector3f (map_struct.h:201,212): Eigen 3.3
+// multiplies the 4x4 matrix by (v, 1), each row reduced in halves,
+// (m_i0 v0 + m_i1 v1) + (m_i2 v2 + m_i3); nvcc contracts the first product of
+// each half (measured on the reference's own build).
 __device__ __forceinline__ float3 xf_apply(const Xf& t, float v0, float v1, float v2)
 {
     float3 o;
-    o.x = __fadd_rn(t.m[0][3], __fmaf_rn(t.m[0][0], v0, __fmaf_rn(t.m[0][1], v1, __fmul_rn(t.m[0][2], v2))));
-    o.y = __fadd_rn(t.m[1][3], __fmaf_rn(t.m[1][0], v0, __fmaf_rn(t.m[1][1], v1, __fmul_rn(t.m[1][2], v2))));
-    o.z = __fadd_rn(t.m[2][3], __fmaf_rn(t.m[2][0], v0, __fmaf_rn(t.m[2][1], v1, __fmul_rn(t.m[2][2], v2))));
+    o.x = __fadd_rn(__fmaf_rn(t.m[0][0], v0, __fmul_rn(t.m[0][1], v1)), __fmaf_rn(t.m[0][2], v2, t.m[0][3]));
+    o.y = __fadd_rn(__fmaf_rn(t.m[1][0], v0, __fmul_rn(t.m[1][1], v1)), __fmaf_rn(t.m[1][2], v2, t.m[1][3]));
+    o.z = __fadd_rn(__fmaf_rn(t.m[2][0], v0, __fmul_rn(t.m[2][1], v1)), __fmaf_rn(t.m[2][2], v2, t.m[2][3]));
     return o;
 }
 
@@ -88,10 +90,12 @@ __device__ __forceinline__ float sqnorm(float3 v)
     return __fmaf_rn(v.x, v.x, __fmaf_rn(v.y, v.y, __fmul_rn(v.z, v.z)));
 }
 
-// Eigen normalized(): v / sqrt(|v|^2) if |v|^2 > 0 else v.
+// Eigen normalized(): v / sqrt(|v|^2) if |v|^2 > 0 else v. Inside
+// normalized() nvcc contracts the squared norm's inner sum the other way,
+// v0^2 + (v2^2 + v1^2) (measured on the reference's own build).
 __device__ __forceinline__ float3 normalized(float3 v)
 {
-    const float s = sqnorm(v);
+    const float s = __fmaf_rn(v.x, v.x, __fmaf_rn(v.z, v.z, __fmul_rn(v.y, v.y)));
     if (s > 0.f) {
         const float n = __fsqrt_rn(s);
         v.x = __fdiv_rn(v.x, n);
