@@ -10,9 +10,14 @@ through the library's C ABI (libvmap_b200.so).
 N > 1 is launched with torch.distributed.run: every rank maps its own seeded
 scene (independent maps, no collective on the data path: weak scaling) and
 the timed region is the max over ranks of the summed per-step device times.
---impl reference times the reference algorithm's CPU restatement (the
-reference is CUDA/Eigen/OpenCV code that cannot be built here) on the host
-cores, rank 0 only.
+Before the warm-up, --prefix frames (default 100) are fused untimed, so the
+timed frames see a steady-state map rather than a young one.
+
+--impl reference times the reference algorithm's CPU restatement (the oracle
+port: the reference has no CPU implementation) on the host cores, rank 0
+only, on the same frames; beside it (extra key) the reference's own CUDA
+build, compiled from its sources against project-written Eigen/OpenCV
+subsets (oracle/_ref), timed on the GPU as the plain drop-in comparison.
 """
 import argparse
 import ctypes as C
@@ -40,6 +45,8 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=10)
     p.add_argument("--impl", default="product", choices=["product", "reference"])
+    p.add_argument("--prefix", type=int, default=100,
+                   help="frames fused untimed before the warm-up (steady-state map)")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
@@ -48,11 +55,13 @@ def parse():
     p.add_argument("--batch-steps", type=int, default=0, help="timed batched steps (default: --steps // 4)")
     p.add_argument("--batch-blocks", type=int, default=1 << 17, help="block pool per batched map")
     p.add_argument("--uneven", type=int, default=64, help="maps of the uneven batch (0 skips it)")
-    p.add_argument("--serving", action="store_true",
-                   help="also run the serving sweep (256 sessions, Poisson arrivals, 70/25/5 fuse/raycast/mesh)")
-    p.add_argument("--serving-rates", default="100,200,300,400,600")
+    p.add_argument("--no-serving", action="store_true",
+                   help="skip the serving sweep (256 sessions, Poisson arrivals, 70/25/5 fuse/raycast/mesh)")
+    p.add_argument("--serving-rates", default="600,200",
+                   help="offered requests/s per GPU, one per budget (or one for all), comma-separated")
     p.add_argument("--serving-budgets", default="1.0,0.5", help="device memory budgets, fractions of all sessions' bytes")
-    p.add_argument("--serving-requests", type=int, default=1500)
+    p.add_argument("--serving-requests", type=int, default=600)
+    p.add_argument("--serving-warmup", type=int, default=200)
     p.add_argument("--autotune", action="store_true",
                    help="tune the launch shapes first (else a cached or shipped table, if any, is applied)")
     return p.parse_args()
@@ -117,8 +126,11 @@ def workload_config(wl, args, extra=None):
                        "vertex/normal maps at its pose" % (wl.name, wl.width, wl.height, wl.voxel_size * 1e3,
                                                            int(np.log2(wl.num_entries)), int(np.log2(wl.num_blocks)),
                                                            wl.voxel_format.upper()),
-           "path": "plain single map per GPU", "frames": "%d..%d" % (args.warmup, args.warmup + args.steps - 1),
-           "warmup_frames": "0..%d" % (args.warmup - 1), "l2": "flushed between steps (256 MiB write)",
+           "path": "plain single map per GPU",
+           "frames": "%d..%d" % (args.prefix + args.warmup, args.prefix + args.warmup + args.steps - 1),
+           "prefix_frames": "0..%d fused untimed (steady-state map)" % (args.prefix - 1) if args.prefix else "none",
+           "warmup_frames": "%d..%d" % (args.prefix, args.prefix + args.warmup - 1),
+           "l2": "flushed between steps (256 MiB write)",
            "parallelism": "independent maps per rank" if args.gpus > 1 else "single GPU"}
     if extra:
         cfg.update(extra)
@@ -189,25 +201,32 @@ def gpu_index(local_rank):
 
 
 # -------------------------------------------------------------- CPU baseline
-def cpu_oracle_run(wl, frames, n_threads, seconds=None, steps=None, om=None):
-    """Reference algorithm (FP32 restatement, same voxel format) on the host:
-    fuse, then raycast + normal map, per frame, like one GPU step. Returns the
-    oracle map and per-frame seconds of the two stages."""
+def cpu_oracle_run(wl, frames, n_threads, seconds=None, steps=None, om=None, precision=0, counts=None):
+    """Reference algorithm (the oracle in FP32 reference arithmetic, or FP64,
+    same voxel format) on the host: fuse, then raycast + normal map, per
+    frame, like one GPU step. Returns the oracle map and per-frame seconds of
+    the two stages; with `counts` (a dict of lists) also the frame's visible
+    blocks, the unique blocks its allocation touched (A) and the unique
+    blocks its rays read (U)."""
     from oracle import oracle as O
     from voxelmapping_b200 import synth
     O.set_threads(n_threads)
     if om is None:
         om = O.OracleMap(wl.width, wl.height, wl.K, wl.num_blocks, wl.voxel_size, storage=wl.voxel_format,
-                         max_weight=wl.max_weight, with_color=wl.with_color)
+                         max_weight=wl.max_weight, with_color=wl.with_color, precision=precision)
     st = {"fuse": [], "raycast": []}
     t_start = time.perf_counter()
     for d, rgb, pose in frames:
         t0 = time.perf_counter()
-        om.fuse(synth.depth_to_metres(d, wl.depth_scale), rgb if wl.with_color else None, pose)
+        r = om.fuse(synth.depth_to_metres(d, wl.depth_scale), rgb if wl.with_color else None, pose)
         t1 = time.perf_counter()
         O.compute_normal(om.raycast(pose))
         st["fuse"].append(t1 - t0)
         st["raycast"].append(time.perf_counter() - t1)
+        if counts is not None:
+            counts["visible"].append(r["visible"])
+            counts["alloc_touched"].append(om.last_alloc_blocks())
+            counts["ray_blocks"].append(om.last_raycast_blocks())
         if seconds is not None and time.perf_counter() - t_start > seconds:
             break
         if steps is not None and len(st["fuse"]) >= steps:
@@ -215,19 +234,41 @@ def cpu_oracle_run(wl, frames, n_threads, seconds=None, steps=None, om=None):
     return om, st
 
 
-def cpu_baseline(wl, scene, frames, threads, seconds=None, skip=0, one_thread_frames=2):
-    """The oracle on the host cores: frames/s over `frames` (after `skip`
-    untimed ones) with `threads` threads, per-stage p50 / p99, one mesh
-    extraction of the resulting map, and the next `one_thread_frames` frames
-    on one thread."""
+def oracle_prefix(wl, frames, n_threads, precision=0):
+    """An oracle map with `frames` fused (untimed, fusion only): the same
+    steady-state map the GPU arm's prefix builds."""
     from oracle import oracle as O
-    om, st = cpu_oracle_run(wl, frames, threads, seconds=seconds)
-    used = len(st["fuse"])
+    from voxelmapping_b200 import synth
+    O.set_threads(n_threads)
+    om = O.OracleMap(wl.width, wl.height, wl.K, wl.num_blocks, wl.voxel_size, storage=wl.voxel_format,
+                     max_weight=wl.max_weight, with_color=wl.with_color, precision=precision)
+    for d, rgb, pose in frames:
+        om.fuse(synth.depth_to_metres(d, wl.depth_scale), rgb if wl.with_color else None, pose)
+    return om
+
+
+def cpu_baseline(wl, scene, frames, threads, seconds=None, skip=0, one_thread_frames=2, prefix=0):
+    """The oracle on the host cores, after fusing the first `prefix` frames
+    untimed: frames/s over the next frames (after `skip` untimed ones,
+    bounded by `seconds`) with `threads` threads in the reference's FP32
+    arithmetic, per-stage p50 / p99, the unique blocks allocation touched
+    (A) and rays read (U) per frame, one mesh extraction of the resulting map,
+    the next `one_thread_frames` frames on one thread, and the FP64 accuracy
+    oracle timed the same way on a third of the time."""
+    from oracle import oracle as O
+    ms = lambda xs: {"p50": 1e3 * percentile(xs, 50), "p99": 1e3 * percentile(xs, 99)}  # noqa: E731
+    t0 = time.perf_counter()
+    om = oracle_prefix(wl, frames[:prefix], threads)
+    prefix_s = time.perf_counter() - t0
+    counts = {"visible": [], "alloc_touched": [], "ray_blocks": []}
+    om, st = cpu_oracle_run(wl, frames[prefix:], threads, seconds=seconds, om=om, counts=counts)
+    used = prefix + len(st["fuse"])
     fr = [f + r for f, r in zip(st["fuse"], st["raycast"])][skip:]
-    ms = lambda xs: {"p50": 1e3 * percentile(xs, 50), "p99": 1e3 * percentile(xs, 99)}
     out = {"value": len(fr) / sum(fr), "unit": "frames/s", "cores": threads, "kind": "port",
-           "frames_timed": len(fr), "frame_ms": ms(fr), "fuse_ms": ms(st["fuse"][skip:]),
-           "raycast_normals_ms": ms(st["raycast"][skip:])}
+           "precision": "fp32 (the reference's own arithmetic)", "frames_timed": len(fr), "frame_ms": ms(fr),
+           "fuse_ms": ms(st["fuse"][skip:]), "raycast_normals_ms": ms(st["raycast"][skip:]),
+           "prefix_frames_untimed": prefix, "prefix_fuse_s": prefix_s,
+           "oracle_counts_mean": {k: float(np.mean(v[skip:] or v)) for k, v in counts.items()}}
     t0 = time.perf_counter()
     n, _, _ = om.polygonize()
     out["mesh"] = {"ms": 1e3 * (time.perf_counter() - t0), "triangles": int(n), "threads": threads,
@@ -240,6 +281,109 @@ def cpu_baseline(wl, scene, frames, threads, seconds=None, skip=0, one_thread_fr
                              "raycast_normals_ms": ms(st1["raycast"]),
                              "sample": "frames %d..%d on the same map" % (used, used + len(fr1) - 1)}
         O.set_threads(threads)
+    del om
+    # the FP64 accuracy oracle (the double-precision transcription) on the same frames
+    o64 = oracle_prefix(wl, frames[:prefix], threads, precision=1)
+    _, s64 = cpu_oracle_run(wl, frames[prefix:], threads, seconds=(seconds or 15.0) / 3, om=o64)
+    f64 = [f + r for f, r in zip(s64["fuse"], s64["raycast"])]
+    f64 = f64[skip:] or f64
+    out["fp64"] = {"value": len(f64) / sum(f64), "unit": "frames/s", "cores": threads, "frames_timed": len(f64),
+                   "frame_ms": ms(f64), "fuse_ms": ms(s64["fuse"]), "raycast_normals_ms": ms(s64["raycast"])}
+    return out
+
+
+def reference_cuda_build(args, wl, frames):
+    """The reference's own CUDA build (oracle/_ref: src/*.cu compiled against
+    project-written Eigen/OpenCV subsets) timed on the GPU: the class's path,
+    FuseDepthAndImage (depth in metres + colour) then RenderScene and
+    computeNormal per step, after the same prefix; device time per step with
+    CUDA events on the default stream (the reference synchronises the device
+    between its kernels, which the events include), L2 flushed between
+    steps; and end to end from pinned host buffers (depth + colour in, vertex
+    + normal maps out) with the copies inside the timed region."""
+    try:
+        import torch
+        from oracle import refbuild as RB
+    except Exception as e:  # pragma: no cover - import failure is reported
+        return {"unavailable": "import failed: %s" % e}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+    if not RB.available():
+        return {"unavailable": "reference build missing (make -C oracle ref with the reference sources)"}
+    dev = torch.device("cuda", 0)
+    H, W = wl.height, wl.width
+    nfr = len(frames)
+    depth_m = [torch.from_numpy(f[0].astype(np.float32) * np.float32(wl.depth_scale)).to(dev) for f in frames]
+    rgb_d = [torch.from_numpy(np.ascontiguousarray(f[1])).to(dev) for f in frames]
+    poses = [np.asarray(f[2], np.float32) for f in frames]
+    rm = RB.RefMap(W, H, wl.K, wl.num_entries, wl.num_blocks, wl.voxel_size, with_color=True)
+    lib = RB.lib()
+    vmap = torch.empty((H, W, 4), dtype=torch.float32, device=dev)
+    nmap = torch.empty_like(vmap)
+    flush = torch.empty(FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    pp = [np.ascontiguousarray(p.reshape(16)) for p in poses]
+    pc = [p.ctypes.data_as(C.POINTER(C.c_float)) for p in pp]
+
+    def step(i, d, c):
+        RB._check(lib.ref_fuse(rm._h, d.data_ptr(), W * 4, c.data_ptr(), W * 3, pc[i], 0, None), "ref_fuse")
+        RB._check(lib.ref_render(rm._h, vmap.data_ptr(), W * 16, pc[i]), "ref_render")
+        RB._check(lib.ref_compute_normal(vmap.data_ptr(), W * 16, nmap.data_ptr(), W * 16, W, H), "ref_compute_normal")
+
+    P, K, Wm = args.prefix, args.steps, args.warmup
+    for i in range(P):
+        RB._check(lib.ref_fuse(rm._h, depth_m[i].data_ptr(), W * 4, rgb_d[i].data_ptr(), W * 3, pc[i], 0, None),
+                  "ref_fuse")
+    for i in range(P, P + Wm):
+        step(i, depth_m[i], rgb_d[i])
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    for k in range(K):
+        i = P + Wm + k
+        flush.fill_(k & 255)
+        ev[k][0].record()
+        step(i, depth_m[i], rgb_d[i])
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    ms = [a.elapsed_time(b) for a, b in ev]
+    out = {"value": K / (sum(ms) / 1e3), "unit": "frames/s", "ms_per_step": sum(ms) / K,
+           "p50_ms": percentile(ms, 50), "p99_ms": percentile(ms, 99), "kind": "reference",
+           "path": "reference CUDA sources (src/*.cu) built for sm_100a against Eigen/OpenCV subsets; "
+                   "FuseDepthAndImage + RenderScene (CheckVisibleBlocks, ProjectRenderingBlocks, ray march) + "
+                   "computeNormal per step, VoxelRGB storage (int16 TSDF + uint8 weight + colour)"}
+    # end to end: pinned host depth (float metres, as the reference's API
+    # takes it) + colour in, vertex + normal maps out
+    rm.reset()
+    dh = [t.cpu().pin_memory() for t in depth_m]
+    ch = [t.cpu().pin_memory() for t in rgb_d]
+    vh = torch.empty((H, W, 4), dtype=torch.float32).pin_memory()
+    nh = torch.empty_like(vh).pin_memory()
+    dd, cd = torch.empty_like(depth_m[0]), torch.empty_like(rgb_d[0])
+    for i in range(P):
+        RB._check(lib.ref_fuse(rm._h, depth_m[i].data_ptr(), W * 4, rgb_d[i].data_ptr(), W * 3, pc[i], 0, None),
+                  "ref_fuse")
+
+    def step_host(i):
+        dd.copy_(dh[i], non_blocking=True)
+        cd.copy_(ch[i], non_blocking=True)
+        step(i, dd, cd)
+        vh.copy_(vmap, non_blocking=True)
+        nh.copy_(nmap, non_blocking=True)
+
+    for i in range(P, P + Wm):
+        step_host(i)
+    torch.cuda.synchronize()
+    e2 = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(K)]
+    for k in range(K):
+        flush.fill_(k & 255)
+        e2[k][0].record()
+        step_host(P + Wm + k)
+        e2[k][1].record()
+    torch.cuda.synchronize()
+    ems = [a.elapsed_time(b) for a, b in e2]
+    out["e2e"] = {"value": K / (sum(ems) / 1e3), "unit": "frames/s", "p50_ms": percentile(ems, 50),
+                  "p99_ms": percentile(ems, 99), "h2d_bytes_per_step": W * H * (4 + 3),
+                  "d2h_bytes_per_step": 2 * W * H * 16}
+    rm.close()
     return out
 
 
@@ -250,12 +394,14 @@ def run_reference(args):
     from voxelmapping_b200 import synth
     wl = synth.WORKLOADS[WORKLOAD]
     scene = synth.Scene(wl)
-    frames = [scene.render(i) for i in range(args.warmup + args.steps)]
+    frames = [scene.render(i) for i in range(args.prefix + args.warmup + args.steps)]
     threads = os.cpu_count() or 1
-    cb = cpu_baseline(wl, scene, frames, threads, skip=args.warmup)
+    cb = cpu_baseline(wl, scene, frames, threads, skip=args.warmup, prefix=args.prefix)
     value = cb["value"]
-    cb["sample"] = ("frames %d..%d of %s, fuse + raycast + normals each (every step a full frame)"
-                    % (args.warmup, args.warmup + args.steps - 1, WORKLOAD))
+    cb["sample"] = ("frames %d..%d of %s after %d untimed prefix frames, fuse + raycast + normals each (every "
+                    "step a full frame), FP32 reference arithmetic" % (args.prefix + args.warmup,
+                                                                       args.prefix + args.warmup + args.steps - 1,
+                                                                       WORKLOAD, args.prefix))
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / value,
             "p50_ms": cb["frame_ms"]["p50"], "p99_ms": cb["frame_ms"]["p99"],
@@ -264,6 +410,10 @@ def run_reference(args):
             "config": workload_config(wl, args, {"path": "reference algorithm, CPU restatement (oracle port)"}),
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    try:
+        line["reference_cuda_build"] = reference_cuda_build(args, wl, frames)
+    except Exception as e:  # reported, not fatal: the CPU port is the arm's value
+        line["reference_cuda_build"] = {"unavailable": "failed: %s" % e}
     print(json.dumps(line), flush=True)
 
 
@@ -436,13 +586,17 @@ def batched_same_size(args, wl, rank):
 
 def batched_uneven(args, rank):
     """args.uneven maps of uneven extent U(1,8) m, voxel size {4,8,12,16} mm,
-    resolution {320x240, 640x480, 1280x720}, pools 2^14..2^19, FP16 + colour."""
+    resolution {320x240, 640x480, 1280x720}, pools 2^14..2^19, FP16 + colour.
+    Each pool is twice the generator's surface-area estimate (capped at 2^19
+    blocks), so that no map runs out of blocks over the timed frames."""
+    import dataclasses
     from voxelmapping_b200 import synth
-    wls = synth.uneven_workloads(args.uneven, seed=rank + 1)
+    wls = [dataclasses.replace(w, num_blocks=min(2 * w.num_blocks, 1 << 19), num_entries=min(2 * w.num_entries, 1 << 21))
+           for w in synth.uneven_workloads(args.uneven, seed=rank + 1)]
     desc = ("%d maps of uneven extent U(1,8) m, voxel size {4,8,12,16} mm, depth resolution {320x240, 640x480, "
-            "1280x720}, pools 2^14..2^19 blocks, FP16 TSDF + uint16 weight (cap 128) + uint8x3 colour, each its own "
-            "seeded scene; one step = one frame per map fused + raycast in one vmap_batch_step; each map cycles "
-            "through 8 rendered frames; L2 flushed between steps" % args.uneven)
+            "1280x720}, pools 2^14..2^19 blocks (twice the surface-area estimate), FP16 TSDF + uint16 weight (cap 128) "
+            "+ uint8x3 colour, each its own seeded scene; one step = one new frame per map (consecutive poses) fused + "
+            "raycast in one vmap_batch_step; L2 flushed between steps" % args.uneven)
     return wls, desc
 
 
@@ -466,7 +620,8 @@ def run_product(args):
         wl = dataclasses.replace(wl, num_blocks=args.num_blocks)
     wl_r = dataclasses.replace(wl, seed=wl.seed + rank)
     scene = synth.Scene(wl_r)
-    nfr = args.warmup + args.steps
+    P0 = args.prefix
+    nfr = P0 + args.warmup + args.steps
     frames = [scene.render(i) for i in range(nfr)]
     depth_d = torch.from_numpy(np.stack([f[0] for f in frames]).view(np.int16)).to(dev)
     rgb_d = torch.from_numpy(np.stack([f[1] for f in frames])).to(dev).reshape(nfr, wl.height, wl.width * 3)
@@ -484,10 +639,19 @@ def run_product(args):
     h = vm._map
     vpitch = wl.width * 16
 
-    def step(i):
+    def fuse_only(i):
         L.check(lib.vmap_fuse_depth_rgb(h, depth_d[i].data_ptr(), L.DEPTH_U16, wl.width * 2, wl.depth_scale,
                                         rgb_d[i].data_ptr(), wl.width * 3, poses[i], sp))
+
+    def step(i):
+        fuse_only(i)
         L.check(lib.vmap_render_scene(h, poses[i], vmap.data_ptr(), vpitch, nmap.data_ptr(), vpitch, sp))
+
+    def prefix():
+        """Frames 0 .. prefix-1 fused untimed: a steady-state map."""
+        for i in range(P0):
+            fuse_only(i)
+        torch.cuda.synchronize()
 
     def tune():
         # on a scratch map of the same configuration, so the timed map's
@@ -509,8 +673,9 @@ def run_product(args):
     from voxelmapping_b200 import autotune as AT
     launch_cfg, tune_src = apply_tuning(vm, AT.key_for("map", wl.voxel_format, wl.width, wl.height), args, tune)
 
+    prefix()
     for i in range(args.warmup):
-        step(i)
+        step(P0 + i)
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -523,7 +688,7 @@ def run_product(args):
     for k in range(args.steps):
         flush.fill_(k & 255)
         ev[k][0].record()
-        step(args.warmup + k)
+        step(P0 + args.warmup + k)
         ev[k][1].record()
         L.check(lib.vmap_copy_counters(h, counters[k].data_ptr(), sp))
     torch.cuda.synchronize()
@@ -542,27 +707,13 @@ def run_product(args):
     vis = cnt[:, 1].astype(np.float64)
     alloc = np.minimum(cnt[:, 0], wl.num_blocks).astype(np.float64)
 
-    # --- roofline: algorithmic bytes per launch of each stage (bench model) --
+    # stage timings now; their algorithmic bytes (and the roofline) once the
+    # CPU leg has counted the oracle's U and A on the same frames
     P = wl.width * wl.height
     s_vox = L.lib().vmap_block_bytes(L.FORMAT_NAMES[wl.voxel_format], int(wl.with_color)) / 512.0
-    s_tsdf = {"ref": 3, "f32": 8, "f16": 4, "i16": 4}[wl.voxel_format]
-    stage_bytes = {
-        "alloc": P * 2 + vis.mean() * 32,                         # depth read + one probe sector per block
-        "visibility": alloc.mean() * 8 + vis.mean() * 4,          # block keys + visible list
-        "fuse": vis.mean() * (512 * s_vox * 2 + 12) + P * 5,      # block RMW + depth/colour images
-        "zrange": alloc.mean() * 8,
-        "raycast": vis.mean() * 512 * s_tsdf + P * 16,            # touched blocks' tsdf+weight + vertex map
-        "normals": P * 32,
-    }
-    stages = {}
-    for i, name in enumerate(L.STAGES):
-        if stage_n[i]:
-            per = stage_ms[i] / stage_n[i]
-            b = stage_bytes.get(name)
-            stages[name] = {"launches": int(stage_n[i]), "ms_per_launch": per,
-                            "share": stage_ms[i] / max(sum(stage_ms), 1e-9),
-                            "alg_bytes": b, "gbs": (b / (per * 1e-3) / 1e9) if b else None}
-    dom = max(stages, key=lambda k: stages[k]["ms_per_launch"] * stages[k]["launches"])
+    s_tsdf = {"ref": 4, "f32": 8, "f16": 4, "i16": 4}[wl.voxel_format]  # the voxel word rays read
+    stage_time = {name: (int(stage_n[i]), stage_ms[i] / stage_n[i]) for i, name in enumerate(L.STAGES) if stage_n[i]}
+    total_stage_ms = max(sum(stage_ms), 1e-9)
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
@@ -570,29 +721,12 @@ def run_product(args):
     peak = peaks.get("hbm_gbs")
     peak_src = "measured" if peak else "fallback"
     peak = peak or 6650.0
-    traffic, l2_pct, traffic_capture, scale = None, None, None, None
-    tf = ROOT / "profiles" / "ncu_traffic.json"
-    if tf.exists():
-        entry = json.loads(tf.read_text()).get(dom, {})
-        traffic_capture, l2_pct = entry.get("dram_bytes_per_launch"), entry.get("l2_throughput_pct")
-        # the capture is a smaller frame: scale its DRAM bytes to this run's
-        # launches by the units the kernel processes (visible blocks)
-        units = entry.get("visible_blocks_at_capture")
-        if traffic_capture is not None and units:
-            scale = float(vis.mean()) / units
-            traffic = traffic_capture * scale
-    roof = {"kernel": dom, "bound": "hbm", "achieved": stages[dom]["gbs"], "peak": peak, "peak_source": peak_src,
-            "unit": "GB/s", "frac": stages[dom]["gbs"] / peak, "traffic": traffic,
-            "alg_bytes_per_launch": stages[dom]["alg_bytes"],
-            "traffic_at_capture": traffic_capture, "traffic_scale": scale,
-            # a latency-bound kernel: its L2 throughput (% of peak, one ncu capture) beside the HBM fraction
-            "l2_throughput_pct_ncu": l2_pct}
 
     line = {"metric": METRIC, "value": value, "unit": "frames/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_total_ms / args.steps,
             "p50_ms": percentile(step_ms, 50), "p99_ms": percentile(step_ms, 99), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": wl.voxel_format, "data": "synthetic",
-            "config": workload_config(wl, args), "roofline": roof, "stages": stages,
+            "config": workload_config(wl, args), "roofline": None, "stages": None,
             "gpu_launches": int(sum(stage_n)),
             "launch_config": launch_cfg, "tuning": tune_src,
             "map": {"allocated_blocks": int(st["allocated_blocks"]), "visible_blocks_mean": float(vis.mean()),
@@ -633,6 +767,7 @@ def run_product(args):
         vmap_h = torch.empty((wl.height, wl.width, 4), dtype=torch.float32).pin_memory()
         nmap_h = torch.empty_like(vmap_h).pin_memory()
         vm.reset()
+        prefix()
 
         def step_host(i):
             L.check(lib.vmap_fuse_host(h, depth_h[i].data_ptr(), L.DEPTH_U16, wl.depth_scale, rgb_h[i].data_ptr(),
@@ -640,7 +775,7 @@ def run_product(args):
             L.check(lib.vmap_render_scene_host(h, poses[i], vmap_h.data_ptr(), nmap_h.data_ptr(), sp))
 
         for i in range(args.warmup):
-            step_host(i)
+            step_host(P0 + i)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
@@ -649,7 +784,7 @@ def run_product(args):
         for k in range(args.steps):
             flush.fill_(k & 255)
             ev2[k][0].record()
-            step_host(args.warmup + k)
+            step_host(P0 + args.warmup + k)
             ev2[k][1].record()
         torch.cuda.synchronize()
         e_ms = [a.elapsed_time(b) for a, b in ev2]
@@ -662,6 +797,7 @@ def run_product(args):
         # the pipelined host path: copies of neighbouring frames overlap each
         # other's kernels; the whole run is timed, L2 flush included
         vm.reset()
+        prefix()
         outs = [(torch.empty((wl.height, wl.width, 4), dtype=torch.float32).pin_memory(),
                  torch.empty((wl.height, wl.width, 4), dtype=torch.float32).pin_memory()) for _ in range(2)]
         hframes = []
@@ -673,7 +809,7 @@ def run_product(args):
             f.vmap_host, f.nmap_host = outs[i & 1][0].data_ptr(), outs[i & 1][1].data_ptr()
             hframes.append(f)
         for i in range(args.warmup):
-            L.check(lib.vmap_frame_host_async(h, C.byref(hframes[i]), sp))
+            L.check(lib.vmap_frame_host_async(h, C.byref(hframes[P0 + i]), sp))
         L.check(lib.vmap_host_wait(h, sp))
         torch.cuda.synchronize()
         if world > 1:
@@ -687,7 +823,7 @@ def run_product(args):
         t0.record()
         for k in range(args.steps):
             flush.fill_(k & 255)
-            L.check(lib.vmap_frame_host_async(h, C.byref(hframes[args.warmup + k]), sp))
+            L.check(lib.vmap_frame_host_async(h, C.byref(hframes[P0 + args.warmup + k]), sp))
         L.check(lib.vmap_host_wait(h, sp))
         t1.record()
         torch.cuda.synchronize()
@@ -710,7 +846,7 @@ def run_product(args):
         line["batched"]["config"] = desc
     if args.uneven > 0:
         wls, desc = batched_uneven(args, rank)
-        line["batched_uneven"] = run_batched(args, wls, dev, flush, world, distinct_frames=8)
+        line["batched_uneven"] = run_batched(args, wls, dev, flush, world)
         line["batched_uneven"]["config"] = desc
 
     clk.__exit__(None, None, None)
@@ -720,11 +856,71 @@ def run_product(args):
     # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cb = cpu_baseline(wl, scene, frames, threads, seconds=args.cpu_seconds)
-        cb["sample"] = ("frames 0..%d of %s (fuse + raycast + normals each, FP32 reference-algorithm "
-                        "restatement, %d threads)" % (cb["frames_timed"] - 1, WORKLOAD, threads))
+        cb = cpu_baseline(wl, scene, frames, threads, seconds=args.cpu_seconds, prefix=args.prefix)
+        cb["sample"] = ("frames %d..%d of %s after %d untimed prefix frames (fuse + raycast + normals each, FP32 "
+                        "reference-algorithm restatement, %d threads; FP64 beside)"
+                        % (args.prefix, args.prefix + cb["frames_timed"] - 1, WORKLOAD, args.prefix, threads))
         line["cpu_baseline"] = cb
-    if args.serving:
+    # --- roofline: algorithmic bytes per launch of each stage ---------------
+    # P pixels, V visible blocks and B allocated blocks (device counters of the
+    # timed steps), A blocks the allocation touched and U blocks rays read
+    # (the oracle's counts on the same frames, when the CPU leg ran; else the
+    # visible blocks stand in, an upper bound), S bytes per voxel (word +
+    # colour), S_w the word rays read; hash bucket 64 B, block key 8 B, list
+    # entry 4 B.
+    oc = (line.get("cpu_baseline") or {}).get("oracle_counts_mean")
+    V, B = float(vis.mean()), float(alloc.mean())
+    A = oc["alloc_touched"] if oc else V
+    U = oc["ray_blocks"] if oc else V
+    src = "oracle counts on the same frames" if oc else "visible blocks (no oracle count: upper bound)"
+    stage_bytes = {
+        "alloc": P * 2 + A * 64,                          # depth + one bucket probe per touched block
+        "visibility": B * 8 + V * 4,                      # block keys + visible list
+        "fuse": V * (512 * s_vox * 2 + 4 + 8) + P * 5,    # block RMW + list + key + depth/colour
+        "zrange": B * 8,
+        "raycast": U * 512 * s_tsdf + P * 16,             # blocks rays read + vertex map
+        "normals": P * 32,
+    }
+    stages = {}
+    for name, (n_l, per) in stage_time.items():
+        bts = stage_bytes.get(name)
+        g = bts / (per * 1e-3) / 1e9 if bts else None
+        stages[name] = {"launches": n_l, "ms_per_launch": per, "share": n_l * per / total_stage_ms,
+                        "alg_bytes": bts, "gbs": g, "frac": g / peak if g else None}
+    # whole-frame aggregates: the fused frame
+    # P(2+3) + A E_alloc + B E_list + 2 V 512 S + 4 V, the rendered frame
+    # U 512 S_w + P 32 (vertex + normal maps)
+    agg = {"fused_frame": (("alloc", "visibility", "fuse"),
+                           P * 5 + A * 64 + B * 8 + V * 512 * s_vox * 2 + V * 4),
+           "rendered_frame": (("zrange", "raycast", "normals"), U * 512 * s_tsdf + P * 32)}
+    for name, (parts, bts) in agg.items():
+        t = sum(stages[p_]["ms_per_launch"] for p_ in parts if p_ in stages)
+        g = bts / (t * 1e-3) / 1e9
+        stages[name] = {"stages": list(parts), "ms": t, "alg_bytes": bts, "gbs": g, "frac": g / peak}
+    dom = max(stage_time, key=lambda k: stage_time[k][0] * stage_time[k][1])
+    traffic, l2_pct, traffic_capture, scale = None, None, None, None
+    tf = ROOT / "profiles" / "ncu_traffic.json"
+    if tf.exists():
+        entry = json.loads(tf.read_text()).get(dom, {})
+        traffic_capture, l2_pct = entry.get("dram_bytes_per_launch"), entry.get("l2_throughput_pct")
+        # the capture is a smaller frame: scale its DRAM bytes to this run's
+        # launches by the units the kernel processes
+        units = entry.get("units_at_capture") or entry.get("visible_blocks_at_capture")
+        unit_now = U if entry.get("units_at_capture") else V
+        if traffic_capture is not None and units:
+            scale = float(unit_now) / units
+            traffic = traffic_capture * scale
+    line["roofline"] = {"kernel": dom, "bound": "hbm", "achieved": stages[dom]["gbs"], "peak": peak,
+                        "peak_source": peak_src, "unit": "GB/s", "frac": stages[dom]["frac"], "traffic": traffic,
+                        "alg_bytes_per_launch": stages[dom]["alg_bytes"], "units": {"P": P, "V": V, "B": B,
+                                                                                   "A": A, "U": U, "source": src},
+                        "traffic_at_capture": traffic_capture, "traffic_scale": scale,
+                        # a latency-bound kernel: its L2 throughput (% of peak, one ncu capture) beside
+                        "l2_throughput_pct_ncu": l2_pct}
+    line["stages"] = stages
+    line["mesh"]["emit_frac_of_peak"] = line["mesh"]["emit_gbs"] / peak
+
+    if not args.no_serving:
         from voxelmapping_b200 import serving as S
         rates = [float(r) for r in args.serving_rates.split(",")]
         line["serving"] = {"config": "256 sessions per GPU of uneven extent / voxel size / resolution (FP16 + "
@@ -735,20 +931,50 @@ def run_product(args):
                                      "meshes their triangles; latency = completion - arrival, wall clock; summaries "
                                      "merged over the ranks" % args.serving_requests, "runs": []}
         gather = lambda x: all_gather_objects(x, world)  # noqa: E731
-        for frac in [float(b) for b in args.serving_budgets.split(",")]:
-            res, ex = S.run_serving(n_sessions=256, rates=rates, count=args.serving_requests, budget_frac=frac,
-                                    warmup=500, seed=0, rank=rank, world=world, all_gather=gather)
+        budgets = [float(b) for b in args.serving_budgets.split(",")]
+        for bi, frac in enumerate(budgets):
+            # one rate per budget when as many are given, else every rate at every budget
+            rts = [rates[bi]] if len(rates) == len(budgets) else rates
+            res, ex = S.run_serving(n_sessions=256, rates=rts, count=args.serving_requests, budget_frac=frac,
+                                    warmup=args.serving_warmup, seed=0, rank=rank, world=world, all_gather=gather)
             ex.release()
             parts = gather(res)
             for k in range(len(res)):
                 r = S.merge_summaries([p[k] for p in parts])
                 r["budget_frac"] = frac
                 line["serving"]["runs"].append({key: v for key, v in r.items() if not key.startswith("_")})
+    line["headline"] = headline(line)
     if rank == 0:
         print(json.dumps(line), flush=True)
     vm.release()
     if world > 1:
         dist.destroy_process_group()
+
+
+def headline(line):
+    """The numbers a reader looks for first, compact, as the line's last key."""
+    r = lambda x, n=3: None if x is None else round(float(x), n)  # noqa: E731
+    h = {"plain_fps": r(line["value"], 1), "plain_p50_ms": r(line["p50_ms"]), "plain_p99_ms": r(line["p99_ms"]),
+         "e2e_fps": r((line.get("e2e") or {}).get("value"), 1),
+         "raycast_roofline_frac": r((line.get("roofline") or {}).get("frac"), 4)}
+    for arm in ("batched", "batched_uneven"):
+        b = line.get(arm)
+        if b:
+            h[arm] = {"fps": r(b["value"], 1), "plain_same_frames_fps": r(b["plain_same_frames"]["value"], 1),
+                      "ratio_vs_plain": r(b["ratio_vs_plain"]), "p50_ms_per_step": r(b["p50_ms_per_step"]),
+                      "p99_ms_per_step": r(b["p99_ms_per_step"]), "maps_pool_full": b["maps_pool_full"]}
+    sv = line.get("serving")
+    if sv:
+        h["serving"] = [{"budget": x.get("budget_frac"), "offered_rps": r(x.get("offered_rps"), 1),
+                         "served_rps": r(x.get("throughput_rps"), 1),
+                         "p50_ms": {k: r(x[k]["p50_ms"], 2) for k in ("fuse", "raycast", "mesh") if k in x},
+                         "p99_ms": {k: r(x[k]["p99_ms"], 2) for k in ("fuse", "raycast", "mesh") if k in x}}
+                        for x in sv["runs"]]
+    cb = line.get("cpu_baseline")
+    if cb:
+        h["cpu_fp32_fps"] = r(cb["value"], 2)
+        h["cpu_fp64_fps"] = r((cb.get("fp64") or {}).get("value"), 2)
+    return h
 
 
 def main():

@@ -1,6 +1,8 @@
 """`bench.py --impl reference` on CPU: the oracle port on the host cores prints
 one JSON line with the bench contract's keys, the per-stage CPU times (fuse,
-raycast + normals, mesh) and a one-thread sample."""
+raycast + normals, mesh), a one-thread sample, the FP64 oracle beside, the
+oracle's block counts, and the reference CUDA build's entry (unavailable
+without a GPU)."""
 import json
 import os
 import subprocess
@@ -12,7 +14,8 @@ ROOT = Path(__file__).resolve().parent.parent
 
 def test_reference_arm_prints_one_contract_line():
     env = {k: v for k, v in os.environ.items() if k not in ("RANK", "WORLD_SIZE", "LOCAL_RANK")}
-    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "2", "--warmup", "1"],
+    out = subprocess.run([sys.executable, "bench.py", "--impl", "reference", "--steps", "2", "--warmup", "1",
+                          "--prefix", "3"],
                          cwd=ROOT, env=env, capture_output=True, text=True, timeout=600)
     assert out.returncode == 0, out.stderr[-2000:]
     lines = [l for l in out.stdout.splitlines() if l.strip()]
@@ -22,7 +25,11 @@ def test_reference_arm_prints_one_contract_line():
     assert line["steps"] == 2 and line["warmup"] == 1 and line["value"] > 0
     cb = line["cpu_baseline"]
     assert cb["kind"] == "port" and cb["cores"] >= 1 and cb["value"] == line["value"]
-    assert cb["frames_timed"] == 2 and "frames 1..2" in cb["sample"]
+    assert cb["frames_timed"] == 2 and "frames 4..5" in cb["sample"] and cb["prefix_frames_untimed"] == 3
+    assert cb["fp64"]["value"] > 0 and set(cb["oracle_counts_mean"]) == {"visible", "alloc_touched", "ray_blocks"}
+    assert 0 < cb["oracle_counts_mean"]["ray_blocks"] <= cb["oracle_counts_mean"]["visible"]
+    assert "unavailable" in line["reference_cuda_build"] or line["reference_cuda_build"]["value"] > 0
+    assert line["config"]["frames"] == "4..5"
     for k in ("frame_ms", "fuse_ms", "raycast_normals_ms"):
         assert 0 < cb[k]["p50"] <= cb[k]["p99"]
     assert cb["mesh"]["triangles"] > 0 and cb["mesh"]["ms"] > 0

@@ -226,15 +226,21 @@ def test_complete_allocation_room_small_all_frames():
     assert np.abs(p_g - p_r)[inner].max() <= 1
     # marching cubes over the whole map
     n_g, v_g, nn_g = vm.Polygonize()
-    n_r, v_rr, nn_r, _ = rm.polygonize(n_g + 1024)
-    print("triangles: library %d, reference %d" % (n_g, n_r))
+    n_r, v_rr, nn_r, _ = rm.polygonize(int(n_g * 1.5) + 1024)
     info = rm.info()
     if (last_bucket_mask(vm.export_blocks(with_rgb=False)["coords"], info["buckets"])).any():
         pytest.skip("a block of the last bucket is missing from the reference build; mesh not comparable")
-    assert n_g == n_r > 10000
-    a = sorted_rows(np.concatenate([v_g, nn_g], axis=1))
-    b = sorted_rows(np.concatenate([v_rr, nn_r], axis=1))
-    assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+    # the reference polygonizes every hash entry (select_blocks,
+    # marching_cubes.cu:25-50), duplicates of a block included, so its
+    # triangles are the library's, some of them repeated: equal as sets
+    a = np.unique(np.concatenate([v_g, nn_g], axis=1).view(np.uint32), axis=0)
+    b = np.unique(np.concatenate([v_rr, nn_r], axis=1).view(np.uint32), axis=0)
+    dups = len(rm.export()["coords"]) - len(np.unique(block_keys(rm.export()["coords"])))
+    print("triangles: library %d (%d distinct), reference %d (%d distinct), duplicate entries %d" %
+          (n_g, len(a), n_r, len(b), dups))
+    assert n_g > 10000 and n_r < int(n_g * 1.5) + 1024 and n_r >= n_g
+    assert np.array_equal(a, b)
+    assert n_r == n_g or dups > 0
 
 
 def test_complete_allocation_with_colour_room_small():
