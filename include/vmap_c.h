@@ -271,6 +271,12 @@ typedef struct vmap_launch_config {
      * from both ends. Tiles are independent, so only the time changes: the
      * slowest tiles are best started first. */
     int raycast_tile_order;
+    /* ray-marcher tile: a warp marches a tile of 32 neighbouring rays,
+     * raycast_tile_width pixels wide (4, 8 or 16; 0 = 8) and 32 / width
+     * high; raycast_threads_per_cta is 128 or 256 (0 = 256). Only the time
+     * changes. */
+    int raycast_tile_width;
+    int raycast_threads_per_cta;
 } vmap_launch_config;
 vmap_status vmap_get_launch_config(const vmap_map* map, vmap_launch_config* out);
 vmap_status vmap_set_launch_config(vmap_map* map, const vmap_launch_config* cfg);

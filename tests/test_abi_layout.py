@@ -90,12 +90,14 @@ def expected_map_bytes(w, h, num_entries, num_blocks, fmt, color):
     """Device bytes of one map as documented: hash slots (4 x 16 B per bucket;
     buckets = int(0.9 numVoxels), raised to cover numEntries), block keys,
     voxel pool, 16 counters, visible list, near and far z-range tiles (8x8
-    pixels), a triangle counter; each buffer starts on a 256-byte boundary."""
+    pixels), a triangle counter, 7 forward neighbour links per block; each
+    buffer starts on a 256-byte boundary."""
     nb = max(int(num_blocks * 0.9), 1)
     nb = max(nb, -(-num_entries // 4))
     tiles = -(-w // 8) * -(-h // 8)
     bb = L.lib().vmap_block_bytes(fmt, color)
-    sizes = [nb * 4 * 16, num_blocks * 8, num_blocks * bb, 16 * 4, num_blocks * 4, tiles * 8, tiles * 8, 4]
+    sizes = [nb * 4 * 16, num_blocks * 8, num_blocks * bb, 16 * 4, num_blocks * 4, tiles * 8, tiles * 8, 4,
+             num_blocks * 7 * 4]
     return sum(-(-s // 256) * 256 for s in sizes)
 
 

@@ -28,6 +28,9 @@ def test_store_and_lookup(tmp_path, monkeypatch):
 
 def test_candidates_are_valid_launch_values():
     for f in AT.FIELDS:
-        assert all(0 <= c <= 64 for c in AT.CANDIDATES[f]), f
+        if f.endswith("_ctas_per_sm"):  # grids: 0 (default) .. 64 CTAs per SM
+            assert all(0 <= c <= 64 for c in AT.CANDIDATES[f]), f
     assert set(AT.CANDIDATES["raycast_tile_order"]) == {0, 1, 2}
-    assert set(AT.STAGE) | {"mesh_ctas_per_sm", "raycast_tile_order"} == set(AT.FIELDS)
+    assert set(AT.STAGE) | {"mesh_ctas_per_sm"} | set(AT.RAYCAST_PARAMS) == set(AT.FIELDS)
+    assert set(AT.CANDIDATES["raycast_tile_width"]) == {4, 8, 16}
+    assert set(AT.CANDIDATES["raycast_threads_per_cta"]) == {128, 256}

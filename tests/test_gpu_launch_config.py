@@ -15,8 +15,9 @@ from voxelmapping_b200 import synth
 
 pytestmark = pytest.mark.gpu
 WL = synth.WORKLOADS["room_small"]
-SHAPES = [{}, dict({f: 1 for f in AT.FIELDS}, raycast_tile_order=1),
-          dict({f: 32 for f in AT.FIELDS}, raycast_tile_order=2)]
+GRIDS = [f for f in AT.FIELDS if f.endswith("_ctas_per_sm")]
+SHAPES = [{}, dict({f: 1 for f in GRIDS}, raycast_tile_order=1, raycast_tile_width=16, raycast_threads_per_cta=128),
+          dict({f: 32 for f in GRIDS}, raycast_tile_order=2, raycast_tile_width=4, raycast_threads_per_cta=256)]
 
 
 def new_map(**shape):
@@ -55,7 +56,8 @@ def test_map_results_do_not_depend_on_launch_shape():
 
 def test_invalid_shapes_are_refused():
     vm = new_map()
-    for bad in ({"fuse_ctas_per_sm": 65}, {"raycast_ctas_per_sm": -1}, {"raycast_tile_order": 3}):
+    for bad in ({"fuse_ctas_per_sm": 65}, {"raycast_ctas_per_sm": -1}, {"raycast_tile_order": 3},
+                {"raycast_tile_width": 5}, {"raycast_threads_per_cta": 64}):
         with pytest.raises(L.VmapError):
             vm.set_launch_config(**bad)
     vm.set_launch_config(**{f: 0 for f in AT.FIELDS})  # 0 = defaults
@@ -104,7 +106,7 @@ def test_batch_results_do_not_depend_on_launch_shape_and_tuner_runs():
         L.check(lib.vmap_render_scene(vm._map, L.pose_arg(p), vout.data_ptr(), WL.width * 16, None, 0, s))
     best, table = AT.tune_map(vm, step, n_steps=2, rounds=1, warmup=1)
     # the step renders no normal map: that stage is not tuned
-    assert set(table) == (set(AT.STAGE) - {"normals_ctas_per_sm"}) | {"raycast_tile_order"}
+    assert set(table) == (set(AT.STAGE) - {"normals_ctas_per_sm"}) | set(AT.RAYCAST_PARAMS)
     assert all(best[f] in AT.CANDIDATES[f] for f in table) and best["normals_ctas_per_sm"] == 8
     assert vm.get_launch_config() == best
     m_best, m_table = AT.tune_mesh(vm, rounds=1)

@@ -64,7 +64,8 @@ class LaunchConfig(C.Structure):
     """vmap_launch_config: grid of every stage in CTAs per SM (0 = default)."""
     _fields_ = [("alloc_ctas_per_sm", C.c_int), ("visibility_ctas_per_sm", C.c_int), ("fuse_ctas_per_sm", C.c_int),
                 ("zrange_ctas_per_sm", C.c_int), ("raycast_ctas_per_sm", C.c_int), ("normals_ctas_per_sm", C.c_int),
-                ("mesh_ctas_per_sm", C.c_int), ("raycast_tile_order", C.c_int)]
+                ("mesh_ctas_per_sm", C.c_int), ("raycast_tile_order", C.c_int),
+                ("raycast_tile_width", C.c_int), ("raycast_threads_per_cta", C.c_int)]
 
 
 class SnapshotHeader(C.Structure):

@@ -7,8 +7,10 @@ candidates on the caller's own data and keeps the fastest:
 * a single map (`tune_map`): every trial sets every stage to one candidate and
   reads the per-stage CUDA-event times (vmap_timing_*), so all stages are
   tuned together; candidates are visited round-robin several times and each
-  keeps its median; the ray marcher's tile order is swept afterwards on its
-  own (it shares the stage's time with the stage's grid);
+  keeps its median; then the ray marcher's own parameters, which share the
+  stage's time with its grid, one after another with the rest fixed at their
+  best: the tile shape (width 8, 16 or 4 of a 32-ray tile), threads per CTA
+  (256 or 128) and the tile order;
 * a batch (`tune_batch`): the stages run inside one recorded CUDA graph, so
   the whole step is timed, one stage at a time (coordinate descent);
 * the mesh grid (`tune_mesh`): the counting pass of vmap_polygonize.
@@ -27,7 +29,10 @@ from pathlib import Path
 from . import _lib as L
 
 FIELDS = ["alloc_ctas_per_sm", "visibility_ctas_per_sm", "fuse_ctas_per_sm", "zrange_ctas_per_sm",
-          "raycast_ctas_per_sm", "normals_ctas_per_sm", "mesh_ctas_per_sm", "raycast_tile_order"]
+          "raycast_ctas_per_sm", "normals_ctas_per_sm", "mesh_ctas_per_sm", "raycast_tile_order",
+          "raycast_tile_width", "raycast_threads_per_cta"]
+# the ray marcher's parameters besides its grid, swept one at a time
+RAYCAST_PARAMS = ["raycast_tile_width", "raycast_threads_per_cta", "raycast_tile_order"]
 STAGE = {"alloc_ctas_per_sm": "alloc", "visibility_ctas_per_sm": "visibility", "fuse_ctas_per_sm": "fuse",
          "zrange_ctas_per_sm": "zrange", "raycast_ctas_per_sm": "raycast", "normals_ctas_per_sm": "normals"}
 CANDIDATES = {
@@ -39,6 +44,8 @@ CANDIDATES = {
     "normals_ctas_per_sm": [2, 4, 8, 16],
     "mesh_ctas_per_sm": [4, 8, 16, 32],
     "raycast_tile_order": [0, 1, 2],  # bottom rows first, top rows first, alternating ends
+    "raycast_tile_width": [8, 16, 4],  # 8x4, 16x2 or 4x8 rays per warp
+    "raycast_threads_per_cta": [256, 128],
 }
 SHIPPED = Path(__file__).resolve().parent / "tuning_b200.json"
 
@@ -128,27 +135,29 @@ def tune_map(vm, step, n_steps, rounds=3, warmup=3):
         if med:  # a stage the step never runs (a render without normals) keeps its shape
             table[f] = med
             best[f] = min(med, key=med.get)
-    # the tile order, with the other shapes fixed at their best
-    f, i = "raycast_tile_order", L.STAGES.index("raycast")
-    orders = {c: [] for c in CANDIDATES[f]}
-    for _ in range(rounds):
-        for c in orders:
-            vm.set_launch_config(**dict(best, **{f: c}))
-            L.check(lib.vmap_timing_enable(vm._map, 8 * n_steps))
-            for _ in range(n_steps):
-                step(it)
-                it += 1
-            torch.cuda.synchronize()
-            ms = (C.c_double * 7)()
-            cnt = (C.c_uint32 * 7)()
-            L.check(lib.vmap_timing_read(vm._map, ms, cnt))
-            L.check(lib.vmap_timing_enable(vm._map, 0))
-            if cnt[i]:
-                orders[c].append(ms[i] / cnt[i])
-    med = {c: statistics.median(v) for c, v in orders.items() if v}
-    if med:
-        table[f] = med
-        best[f] = min(med, key=med.get)
+    # the ray marcher's tile shape, threads per CTA and tile order, one at a
+    # time with the other shapes fixed at their best
+    i = L.STAGES.index("raycast")
+    for f in RAYCAST_PARAMS:
+        times = {c: [] for c in CANDIDATES[f]}
+        for _ in range(rounds):
+            for c in times:
+                vm.set_launch_config(**dict(best, **{f: c}))
+                L.check(lib.vmap_timing_enable(vm._map, 8 * n_steps))
+                for _ in range(n_steps):
+                    step(it)
+                    it += 1
+                torch.cuda.synchronize()
+                ms = (C.c_double * 7)()
+                cnt = (C.c_uint32 * 7)()
+                L.check(lib.vmap_timing_read(vm._map, ms, cnt))
+                L.check(lib.vmap_timing_enable(vm._map, 0))
+                if cnt[i]:
+                    times[c].append(ms[i] / cnt[i])
+        med = {c: statistics.median(v) for c, v in times.items() if v}
+        if med:
+            table[f] = med
+            best[f] = min(med, key=med.get)
     vm.set_launch_config(**best)
     return best, table
 

@@ -222,6 +222,7 @@ void free_all(vmap_map* m)
         cudaFree(m->zmin);
         cudaFree(m->zmax);
         cudaFree(m->dNtri);
+        cudaFree(m->dm.nbr);
     }
     cudaFree(m->dDepth);
     cudaFree(m->dRgb);
@@ -357,7 +358,7 @@ vmap_status resolve_config(const vmap_config* cfg_in, vmap_config& cfg)
 // hash slots, block keys, voxel pool, counters, visible list, z-range tiles
 // (min, max), triangle count.
 struct MapLayout {
-    enum { SLOTS, KEYS, POOL, CTR, VIS, ZMIN, ZMAX, NTRI, N };
+    enum { SLOTS, KEYS, POOL, CTR, VIS, ZMIN, ZMAX, NTRI, NBR, N };
     size_t off[N + 1];
 };
 
@@ -369,7 +370,7 @@ MapLayout map_layout(const vmap_config& cfg)
                                      cap * vmap_block_bytes(cfg.voxel_format, cfg.with_color),
                                      C_COUNT * sizeof(unsigned), cap * sizeof(int),
                                      ntiles * sizeof(unsigned long long), ntiles * sizeof(unsigned long long),
-                                     sizeof(unsigned)};
+                                     sizeof(unsigned), cap * 7 * sizeof(int)};
     MapLayout l;
     l.off[0] = 0;
     for (int i = 0; i < MapLayout::N; ++i) l.off[i + 1] = (l.off[i] + sz[i] + 255) / 256 * 256;
@@ -408,7 +409,7 @@ vmap_status build_map(const vmap_config& cfg, unsigned char* base, cudaStream_t 
     const MapLayout l = map_layout(cfg);
     void** ptrs[MapLayout::N] = {(void**)&m->dm.slots, (void**)&m->dm.blockKeys, (void**)&m->dm.pool,
                                  (void**)&m->dm.ctr, (void**)&m->dm.visList, (void**)&m->zmin, (void**)&m->zmax,
-                                 (void**)&m->dNtri};
+                                 (void**)&m->dNtri, (void**)&m->dm.nbr};
     for (int i = 0; i < MapLayout::N; ++i) {
         const size_t bytes = l.off[i + 1] - l.off[i];
         if (base) {

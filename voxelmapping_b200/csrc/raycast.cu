@@ -34,15 +34,50 @@ namespace vmapb {
 // block is a convex combination of its corners, so the box and range bound
 // every ray sample that can fall inside the block. Block 0 also rewinds the
 // raycast work queue for the kernel that follows.
+//
+// The same pass, in both raycast modes, sets the forward neighbour links of
+// the blocks allocated since the last pass, [ctr[C_LINKED], allocated): pool
+// slots are dense, so those are the newest. Each new block is 14 independent
+// tasks spread over the grid, one lookup each: its 7 links, and the link of
+// each of its 7 backward neighbours that points at it. Two new neighbours
+// write each other's link with the same value, so the order of the writes
+// does not matter. The ray marcher, which always follows, reads the links for
+// trilinear corners in neighbouring blocks and advances C_LINKED.
 constexpr float kClipZ = 0.05f;  // below the ray start depth of 0.1 m
+
+__device__ __forceinline__ int links_pending(const MapView& v)
+{
+    if (!v.out.vmap) return 0;
+    const int done = (int)*((volatile const unsigned*)(v.m.ctr + C_LINKED));
+    const int n = allocated_blocks(v.m);
+    return n > done ? 14 * (n - done) : 0;
+}
 
 template <class V>
 __global__ void __launch_bounds__(256) zrange_kernel(V views)
 {
     __shared__ int pre[kMaxBatch + 1];
+    const int nmaps = views.count();
+    // neighbour links of the new blocks
+    map_prefix(views, [](const MapView& v) { return links_pending(v); }, pre);
+    const int ntasks = pre[nmaps];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntasks; i += gridDim.x * blockDim.x) {
+        const int mi = map_of(pre, nmaps, i);
+        const DevMap& m = views[mi].m;
+        const int t = i - pre[mi];
+        const int slot = (int)*((volatile const unsigned*)(m.ctr + C_LINKED)) + t / 14;
+        const int k = 1 + (t % 14) / 2, dx = k & 1, dy = (k >> 1) & 1, dz = (k >> 2) & 1;
+        const int3 b = unpack_key(m.blockKeys[slot]);
+        if (t & 1) {  // a backward neighbour's link to this block
+            const int e = hash_find(m, b.x - dx, b.y - dy, b.z - dz);
+            if (e >= 0) m.nbr[7 * (size_t)e + k - 1] = slot;
+        } else {
+            m.nbr[7 * (size_t)slot + k - 1] = hash_find(m, b.x + dx, b.y + dy, b.z + dz);
+        }
+    }
+    __syncthreads();  // `pre` is reused
     map_prefix(views, [](const MapView& v) { return v.out.vmap && v.out.mode == 0 ? allocated_blocks(v.m) : 0; }, pre);
     if (blockIdx.x == 0 && threadIdx.x == 0) views.queue[0] = 0u;
-    const int nmaps = views.count();
     const int total = pre[nmaps];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const int mi = map_of(pre, nmaps, i);

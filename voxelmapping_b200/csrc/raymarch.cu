@@ -27,13 +27,13 @@
 
 namespace vmapb {
 
-// A warp marches one 8x4-pixel tile: neighbouring rays sample neighbouring
-// voxels at similar depths, so a warp's loads and hash lookups share sectors.
-constexpr int kTileW = 8, kTileH = 4;
-
-__device__ __forceinline__ int ray_tiles(const MapView& v)
+// A warp marches one tile of 32 neighbouring rays (tw x 32/tw pixels, 8 x 4
+// by default): neighbouring rays sample neighbouring voxels at similar
+// depths, so a warp's loads and hash lookups share sectors.
+__device__ __forceinline__ int ray_tiles(const MapView& v, int tw)
 {
-    return v.out.vmap ? ((v.cam.W + kTileW - 1) / kTileW) * ((v.cam.H + kTileH - 1) / kTileH) : 0;
+    const int th = 32 / tw;
+    return v.out.vmap ? ((v.cam.W + tw - 1) / tw) * ((v.cam.H + th - 1) / th) : 0;
 }
 
 __device__ __forceinline__ float3 fma3(float k, float3 d, float3 r)
@@ -142,7 +142,29 @@ struct March {
         return mask;
     }
 
-    // corners across block boundaries: one lookup per distinct block
+    // corners across block boundaries, from the block of corner 0 (slot0)
+    // and its forward neighbour links: floor(p + 1) is floor(p) + 1 or + 2,
+    // so the other corners lie in that block or in a block one step up on
+    // each axis that crosses; the needed links are independent loads
+    static __device__ __forceinline__ bool load8_linked(const DevMap& m, int slot0, const Corners& c, float* s)
+    {
+        const int mask = (vox2blk(c.x1) != vox2blk(c.x0) ? 1 : 0) | (vox2blk(c.y1) != vox2blk(c.y0) ? 2 : 0) |
+                         (vox2blk(c.z1) != vox2blk(c.z0) ? 4 : 0);
+        const int* L = m.nbr + 7 * (size_t)slot0;
+        bool ok = true;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int vx = (k & 1) ? c.x1 : c.x0, vy = (k & 2) ? c.y1 : c.y0, vz = (k & 4) ? c.z1 : c.z0;
+            const int o = k & mask;  // corner k's block, as an offset from corner 0's
+            bool v;
+            s[k] = voxel(m, o ? __ldg(L + o - 1) : slot0, vx, vy, vz, v);
+            ok &= v;
+        }
+        return ok;
+    }
+
+    // corners across block boundaries when corner 0's block is not allocated:
+    // one lookup per distinct block
     static __device__ __forceinline__ bool load8_general(const DevMap& m, Ray& r, const Corners& c, float* s)
     {
         bool ok = true;
@@ -160,12 +182,13 @@ struct March {
     {
         const Corners c = corners(p);
         float s[8];
-        if (c.inner()) {
-            const int slot = block_of(m, r, vox2blk(c.x0), vox2blk(c.y0), vox2blk(c.z0));
-            valid = slot >= 0 ? load8(m, slot, c, s) == 0xffu : false;
-            if (slot < 0)
+        const int slot = block_of(m, r, vox2blk(c.x0), vox2blk(c.y0), vox2blk(c.z0));
+        if (slot >= 0) {
+            valid = c.inner() ? load8(m, slot, c, s) == 0xffu : load8_linked(m, slot, c, s);
+        } else if (c.inner()) {
+            valid = false;
 #pragma unroll
-                for (int k = 0; k < 8; ++k) s[k] = 1.f;
+            for (int k = 0; k < 8; ++k) s[k] = 1.f;
         } else {
             valid = load8_general(m, r, c, s);
         }
@@ -305,7 +328,7 @@ struct March {
                 s[6] = value(w6, v); valid &= v;
                 s[7] = value(w7, v); valid &= v;
             } else {
-                valid = load8_general(m, r, c, s);
+                valid = load8_linked(m, r.cblk, c, s);
             }
             sdf = lerp8(s, c.ax, c.ay, c.az);
         }
@@ -391,14 +414,19 @@ __device__ __forceinline__ int warp_lookup(const DevMap& m, unsigned long long k
 // 4 CTAs per SM (at most 64 registers) measured faster than the 3 that 76
 // registers allow: latency hiding outweighs a small register spill.
 template <class V, int FMT>
-__global__ void __launch_bounds__(256, 4) raycast_kernel(const __grid_constant__ V views, int order)
+__global__ void __launch_bounds__(256, 4) raycast_kernel(const __grid_constant__ V views, int order, int tw)
 {
     typedef March<FMT> M;
     typedef typename M::Corners Corners;
     __shared__ int pre[kMaxBatch + 1];
     __shared__ unsigned long long s_wkey[8][kWarpCache];
     __shared__ int s_wslot[8][kWarpCache];
-    map_prefix(views, [](const MapView& v) { return ray_tiles(v); }, pre);
+    map_prefix(views, [tw](const MapView& v) { return ray_tiles(v, tw); }, pre);
+    // the z-range pass before this launch linked every allocated block of the
+    // maps it renders
+    if (blockIdx.x == 0 && threadIdx.x == 0)
+        for (int mi = 0; mi < views.count(); ++mi)
+            if (views[mi].out.vmap) views[mi].m.ctr[C_LINKED] = (unsigned)allocated_blocks(views[mi].m);
     const int nmaps = views.count();
     const int total = pre[nmaps];
     const int lane = threadIdx.x & 31;
@@ -423,8 +451,8 @@ __global__ void __launch_bounds__(256, 4) raycast_kernel(const __grid_constant__
         // 0 bottom rows first, 1 top rows first, 2 alternating from both ends
         const int q = item - pre[mi], nt = pre[mi + 1] - pre[mi];
         const int t = order == 1 ? q : order == 2 ? ((q & 1) ? nt - 1 - (q >> 1) : (q >> 1)) : nt - 1 - q;
-        const int tx = (v.cam.W + kTileW - 1) / kTileW;
-        const int x = (t % tx) * kTileW + (lane % kTileW), y = (t / tx) * kTileH + (lane / kTileW);
+        const int tx = (v.cam.W + tw - 1) / tw;
+        const int x = (t % tx) * tw + (lane % tw), y = (t / tx) * (32 / tw) + (lane / tw);
         Ray r;
         bool live = x < v.cam.W && y < v.cam.H && M::init(v, r, mi, x, y);
         const bool started = live;
@@ -452,17 +480,27 @@ __global__ void __launch_bounds__(256, 4) raycast_kernel(const __grid_constant__
 template <class V, int FMT>
 static cudaError_t raycast_persistent(const V& views, const Launcher& l, cudaStream_t s)
 {
-    // resident CTAs per SM of this instantiation (a static initialiser runs
-    // once, thread-safely, on the first launch)
-    static const int occ = [] {
-        int o = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, raycast_kernel<V, FMT>, 256, 0) != cudaSuccess || o < 1)
-            o = 1;
-        return o;
-    }();
+    // resident CTAs per SM of this instantiation at 128 and 256 threads (a
+    // static initialiser runs once, thread-safely, on the first launch)
+    static const int occ[2] = {[] {
+                                   int o = 0;
+                                   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, raycast_kernel<V, FMT>, 128,
+                                                                                     0) != cudaSuccess || o < 1)
+                                       o = 1;
+                                   return o;
+                               }(),
+                               [] {
+                                   int o = 0;
+                                   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&o, raycast_kernel<V, FMT>, 256,
+                                                                                     0) != cudaSuccess || o < 1)
+                                       o = 1;
+                                   return o;
+                               }()};
+    const int threads = l.rayThreads == 128 ? 128 : 256;
+    const int fit = occ[threads == 256];
     // CTAs beyond those resident would only start once others finish: cap at occupancy
-    const int per_sm = l.raycast > 0 && l.raycast < occ ? l.raycast : occ;
-    raycast_kernel<V, FMT><<<stage_grid(l, per_sm), 256, 0, s>>>(views, l.tileOrder);
+    const int per_sm = l.raycast > 0 && l.raycast < fit ? l.raycast : fit;
+    raycast_kernel<V, FMT><<<stage_grid(l, per_sm), threads, 0, s>>>(views, l.tileOrder, l.tileW);
     return cudaGetLastError();
 }
 

@@ -40,6 +40,7 @@ enum {
     C_TRI = 3,     // triangles counted by the last polygonize
     C_FAILED = 4,  // allocations refused (pool full)
     C_RAYQ = 8,    // raycast work queue of the single-map path
+    C_LINKED = 9,  // blocks [0, C_LINKED) have their neighbour links set
     C_COUNT = 16
 };
 
@@ -54,6 +55,11 @@ struct DevMap {
     unsigned char* pool;           // capacity * blockBytes
     unsigned* ctr;                 // C_COUNT counters
     int* visList;                  // capacity: visible block slots
+    // forward neighbour links: nbr[7 * s + k - 1] = pool slot of the block at
+    // (bx + (k & 1), by + (k >> 1 & 1), bz + (k >> 2 & 1)) for block slot s,
+    // or -1 while that block is not allocated; set for the blocks below
+    // ctr[C_LINKED] (all of them once a z-range pass has run)
+    int* nbr;                      // capacity * 7
     unsigned long long bucketMagic;  // ceil(2^64 / nBucket): remainder by multiplication
     int nBucket;
     int capacity;

@@ -25,6 +25,8 @@ struct Launcher {
     int raycast = 0;  // persistent ray marcher: 0 = as many CTAs as fit on an SM
     int normals = 8, mesh = 8;
     int tileOrder = 0;  // ray-marcher tile order (vmap_launch_config.raycast_tile_order)
+    int tileW = 8;       // ray-marcher tile width; the tile is 32 rays
+    int rayThreads = 256;  // ray-marcher threads per CTA
 };
 
 // vmap_launch_config <-> Launcher (0 in a field: the default)
@@ -34,7 +36,9 @@ inline bool launch_config_ok(const vmap_launch_config* c)
                       c->raycast_ctas_per_sm, c->normals_ctas_per_sm, c->mesh_ctas_per_sm};
     for (int x : v)
         if (x < 0 || x > 64) return false;
-    return c->raycast_tile_order >= 0 && c->raycast_tile_order <= 2;
+    const int tw = c->raycast_tile_width, tt = c->raycast_threads_per_cta;
+    return c->raycast_tile_order >= 0 && c->raycast_tile_order <= 2 && (tw == 0 || tw == 4 || tw == 8 || tw == 16) &&
+           (tt == 0 || tt == 128 || tt == 256);
 }
 
 inline void launch_config_to(const vmap_launch_config* c, Launcher& l)
@@ -48,6 +52,8 @@ inline void launch_config_to(const vmap_launch_config* c, Launcher& l)
     l.normals = c->normals_ctas_per_sm ? c->normals_ctas_per_sm : d.normals;
     l.mesh = c->mesh_ctas_per_sm ? c->mesh_ctas_per_sm : d.mesh;
     l.tileOrder = c->raycast_tile_order;
+    l.tileW = c->raycast_tile_width ? c->raycast_tile_width : d.tileW;
+    l.rayThreads = c->raycast_threads_per_cta ? c->raycast_threads_per_cta : d.rayThreads;
 }
 
 inline void launch_config_from(const Launcher& l, vmap_launch_config* c)
@@ -60,6 +66,8 @@ inline void launch_config_from(const Launcher& l, vmap_launch_config* c)
     c->normals_ctas_per_sm = l.normals;
     c->mesh_ctas_per_sm = l.mesh;
     c->raycast_tile_order = l.tileOrder;
+    c->raycast_tile_width = l.tileW;
+    c->raycast_threads_per_cta = l.rayThreads;
 }
 
 // grid of `per_sm` CTAs per SM, or fewer when there are fewer work items
