@@ -38,31 +38,51 @@ __device__ __forceinline__ int alloc_tiles(const MapView& v)
 // (CreateBlockLineTracingFunctor, depth_fusion.cu:32-59): the band
 // [d - mu/2, d + mu/2] is unprojected to world voxel coordinates, sampled at
 // ceil(2 |far - near|) points and every sampled block is inserted.
-// Consecutive samples in the same block are inserted once and a warp inserts
-// each distinct block once (__match_any_sync), which leaves the resulting
-// block set unchanged. The CTA of item 0 also clears the visible counters the
-// next kernel accumulates into.
+// The samples of a pixel are walked without touching global memory: each
+// block a pixel enters is staged in a CTA-wide shared-memory set, and once
+// the whole tile has been walked its distinct blocks (a few dozen) are
+// inserted into the hash table in parallel, one thread per block. A warp so
+// waits on one table round trip per tile instead of one per sample step, and
+// the resulting block set is the one a per-sample insertion gives. The CTA
+// of item 0 also clears the visible counters the next kernel accumulates
+// into.
+constexpr int kTileSet = 1024;  // open-addressed set of one tile's blocks (8 KB)
+
+// Stage block key (bx, by, bz) in the tile's set; after 32 occupied probes the
+// block goes straight into the hash table, which leaves the block set unchanged.
+__device__ __forceinline__ void stage_block(unsigned long long* set, const DevMap& m, unsigned long long key, int bx,
+                                            int by, int bz)
+{
+    unsigned h = (unsigned)((key * 0x9E3779B97F4A7C15ull) >> 54);
+#pragma unroll 1
+    for (int p = 0; p < 32; ++p) {
+        const unsigned long long cur = atomicCAS(set + h, kEmptyKey, key);
+        if (cur == kEmptyKey || cur == key) return;
+        h = (h + 1) & (kTileSet - 1);
+    }
+    hash_insert(m, bx, by, bz);
+}
+
 template <class V>
 __global__ void __launch_bounds__(256) alloc_kernel(V views)
 {
     __shared__ int pre[kMaxBatch + 1];
-    map_prefix(views, [](const MapView& v) { return alloc_tiles(v); }, pre);
+    __shared__ unsigned long long set[kTileSet];
+    for (int i = threadIdx.x; i < kTileSet; i += blockDim.x) set[i] = kEmptyKey;
+    map_prefix(views, [](const MapView& v) { return alloc_tiles(v); }, pre);  // ends with __syncthreads
     const int nmaps = views.count();
     if (blockIdx.x == 0)
         for (int i = threadIdx.x; i < nmaps; i += blockDim.x)
             if (views[i].in.active) views[i].m.ctr[C_VISIBLE] = 0u;
     const int total = pre[nmaps];
-    const int lane = threadIdx.x & 31;
     for (int item = blockIdx.x; item < total; item += gridDim.x) {
         const int mi = map_of(pre, nmaps, item);
         const MapView& v = views[mi];
         const DevMap& m = v.m;
         const int t = item - pre[mi];
         const int tx = (v.cam.W + 31) >> 5;
-        const int x = (t % tx) * 32 + lane;
+        const int x = (t % tx) * 32 + (threadIdx.x & 31);
         const int y = (t / tx) * 8 + (threadIdx.x >> 5);
-        int n = 0;
-        float px = 0.f, py = 0.f, pz = 0.f, dx = 0.f, dy = 0.f, dz = 0.f;
         if (x < v.cam.W && y < v.cam.H) {
             const float d = read_depth(v.in, x, y);
             if (!(isnan(d) || d < kMinDepth || d > kMaxDepth)) {
@@ -91,43 +111,45 @@ __global__ void __launch_bounds__(256) alloc_kernel(V views)
                             make_float3(__int2float_rn(fx - nx), __int2float_rn(fy - ny), __int2float_rn(fz - nz));
                         const float len = __fsqrt_rn(sqnorm(dir));
                         // (int)ceil(2.0 * len): the double product of a float by 2 is exact
-                        n = __float2int_rz(ceilf(__fmul_rn(2.f, len)));
+                        const int n = __float2int_rz(ceilf(__fmul_rn(2.f, len)));
                         const float den = __int2float_rn(n - 1);
-                        dx = __fdiv_rn(dir.x, den);
-                        dy = __fdiv_rn(dir.y, den);
-                        dz = __fdiv_rn(dir.z, den);
-                        px = __int2float_rn(nx);
-                        py = __int2float_rn(ny);
-                        pz = __int2float_rn(nz);
+                        const float dx = __fdiv_rn(dir.x, den);
+                        const float dy = __fdiv_rn(dir.y, den);
+                        const float dz = __fdiv_rn(dir.z, den);
+                        float px = __int2float_rn(nx), py = __int2float_rn(ny), pz = __int2float_rn(nz);
+                        int lbx = INT_MIN, lby = INT_MIN, lbz = INT_MIN;
+#pragma unroll 1
+                        for (int s = 0; s < n; ++s) {
+                            // pt_start.cast<int>() truncates toward zero, then voxelPosToBlockPos
+                            const int bx = vox2blk(__float2int_rz(px));
+                            const int by = vox2blk(__float2int_rz(py));
+                            const int bz = vox2blk(__float2int_rz(pz));
+                            if (bx != lbx || by != lby || bz != lbz) {  // consecutive samples share blocks
+                                lbx = bx;
+                                lby = by;
+                                lbz = bz;
+                                if (coord_ok(bx, by, bz)) stage_block(set, m, pack_key(bx, by, bz), bx, by, bz);
+                                else atomicOr(m.ctr + C_ERR, VMAP_FLAG_RANGE);
+                            }
+                            px = __fadd_rn(px, dx);
+                            py = __fadd_rn(py, dy);
+                            pz = __fadd_rn(pz, dz);
+                        }
                     }
                 }
             }
         }
-        const unsigned full = 0xffffffffu;
-        const int nmax = __reduce_max_sync(full, n);
-        int lbx = INT_MIN, lby = INT_MIN, lbz = INT_MIN;
-        for (int s = 0; s < nmax; ++s) {
-            unsigned long long key = kEmptyKey;
-            int bx = 0, by = 0, bz = 0;
-            if (s < n) {
-                // pt_start.cast<int>() truncates toward zero, then voxelPosToBlockPos
-                bx = vox2blk(__float2int_rz(px));
-                by = vox2blk(__float2int_rz(py));
-                bz = vox2blk(__float2int_rz(pz));
-                if (bx != lbx || by != lby || bz != lbz) {
-                    lbx = bx;
-                    lby = by;
-                    lbz = bz;
-                    if (coord_ok(bx, by, bz)) key = pack_key(bx, by, bz);
-                    else atomicOr(m.ctr + C_ERR, VMAP_FLAG_RANGE);
-                }
-                px = __fadd_rn(px, dx);
-                py = __fadd_rn(py, dy);
-                pz = __fadd_rn(pz, dz);
+        __syncthreads();
+        // insert the tile's distinct blocks and empty the set for the next tile
+        for (int i = threadIdx.x; i < kTileSet; i += blockDim.x) {
+            const unsigned long long key = set[i];
+            if (key != kEmptyKey) {
+                set[i] = kEmptyKey;
+                const int3 c = unpack_key(key);
+                hash_insert(m, c.x, c.y, c.z);
             }
-            const unsigned peers = __match_any_sync(full, key);
-            if (key != kEmptyKey && (__ffs(peers) - 1) == lane) hash_insert(m, bx, by, bz);
         }
+        __syncthreads();
     }
 }
 
