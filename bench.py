@@ -492,8 +492,6 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
         return step_ms, max_over_ranks(sum(step_ms), dev, world)
 
     # --- batched: one vmap_batch_step over all maps per step
-    maps = make_maps(wls)
-    batch = MapBatch(maps)
     frames = []
     for i in range(nfr):
         fr = (L.BatchFrame * B)()
@@ -508,31 +506,50 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
             f.vmap_dev, f.vmap_pitch = vmaps[b].data_ptr(), w.width * 16
             f.nmap_dev, f.nmap_pitch = nmaps[b].data_ptr(), w.width * 16
         frames.append(fr)
-    def batch_step(i):
-        L.check(lib.vmap_batch_step(batch._h, frames[i % nfr], sp))
-    batch_step.stream = side
-
-    def tune():
-        from voxelmapping_b200 import autotune as AT
-        torch.cuda.synchronize()
-        res = AT.tune_batch(batch, batch_step)
-        torch.cuda.synchronize()
-        for m in maps:  # the timed steps start from empty maps
-            m.reset()
-        torch.cuda.synchronize()
-        return res
     from voxelmapping_b200 import autotune as AT
     key = AT.key_for("batch", wls[0].voxel_format, wls[0].width, wls[0].height, B) if len(
         {(w.width, w.height) for w in wls}) == 1 else AT.key_for("batch", wls[0].voxel_format, 0, 0, B)
-    launch_cfg, tune_src = apply_tuning(batch, key, args, tune)
-    step_ms, tot = timed(batch_step)
-    value = job_throughput(B * K, tot, world)
+
+    def batched(schedule=None):
+        """Fresh maps, the same frames: the tuned launch shapes (schedule None)
+        or those shapes with batch_schedule = schedule."""
+        maps = make_maps(wls)
+        batch = MapBatch(maps)
+
+        def batch_step(i):
+            L.check(lib.vmap_batch_step(batch._h, frames[i % nfr], sp))
+        batch_step.stream = side
+
+        def tune():
+            torch.cuda.synchronize()
+            res = AT.tune_batch(batch, batch_step)
+            torch.cuda.synchronize()
+            for m in maps:  # the timed steps start from empty maps
+                m.reset()
+            torch.cuda.synchronize()
+            return res
+        if schedule is None:
+            launch_cfg, tune_src = apply_tuning(batch, key, args, tune)
+        else:
+            batch.set_launch_config(batch_schedule=schedule)
+            launch_cfg, tune_src = None, None
+        step_ms, tot = timed(batch_step)
+        hits = float(sum(torch.isfinite(v[..., 0]).sum().item() for v in vmaps)) / pixels
+        stats = [m.stats() for m in maps]
+        cfg = batch.get_launch_config()
+        batch.release()
+        for m in maps:
+            m.release()
+        return step_ms, tot, hits, stats, launch_cfg or cfg, tune_src, cfg["batch_schedule"]
+
     pixels = sum(w.width * w.height for w in wls)
-    hits = float(sum(torch.isfinite(v[..., 0]).sum().item() for v in vmaps)) / pixels
-    stats = [m.stats() for m in maps]
-    batch.release()
-    for m in maps:
-        m.release()
+    step_ms, tot, hits, stats, launch_cfg, tune_src, sched = batched()
+    value = job_throughput(B * K, tot, world)
+    # the other schedule on the same frames (1: one launch per stage, 2: one persistent launch)
+    o_ms, o_tot, _, o_stats, _, _, o_sched = batched(3 - sched)
+    other = {"batch_schedule": o_sched, "value": job_throughput(B * K, o_tot, world), "unit": "frames/s",
+             "ms_per_step": o_tot / K, "p50_ms_per_step": percentile(o_ms, 50),
+             "error_flags": int(np.bitwise_or.reduce([s["error_flags"] for s in o_stats]))}
 
     # --- plain: the same frames, FP32 maps, one map per call
     pwls = [dataclasses.replace(w, voxel_format="f32", max_weight=255) for w in wls]
@@ -565,7 +582,7 @@ def run_batched(args, wls, dev, flush, world, distinct_frames=None):
                                   "dtype": "f32",
                                   "path": "FP32 maps, one map per call (vmap_fuse_depth_rgb + vmap_render_scene)"},
             "ratio_vs_plain": value / p_value, "megapixels_per_step": pixels / 1e6, "dtype": wls[0].voxel_format,
-            "launch_config": launch_cfg, "tuning": tune_src,
+            "launch_config": launch_cfg, "tuning": tune_src, "batch_schedule": sched, "other_schedule": other,
             "hit_fraction_last_step": hits, "error_flags": int(np.bitwise_or.reduce([s["error_flags"] for s in stats])),
             "maps_pool_full": int(sum(1 for s in stats if s["error_flags"] & L.FLAG_POOL_FULL)),
             "allocated_blocks_total": int(sum(s["allocated_blocks"] for s in stats))}
@@ -962,7 +979,9 @@ def headline(line):
         if b:
             h[arm] = {"fps": r(b["value"], 1), "plain_same_frames_fps": r(b["plain_same_frames"]["value"], 1),
                       "ratio_vs_plain": r(b["ratio_vs_plain"]), "p50_ms_per_step": r(b["p50_ms_per_step"]),
-                      "p99_ms_per_step": r(b["p99_ms_per_step"]), "maps_pool_full": b["maps_pool_full"]}
+                      "p99_ms_per_step": r(b["p99_ms_per_step"]), "maps_pool_full": b["maps_pool_full"],
+                      "batch_schedule": b.get("batch_schedule"),
+                      "other_schedule_fps": r((b.get("other_schedule") or {}).get("value"), 1)}
     sv = line.get("serving")
     if sv:
         h["serving"] = [{"budget": x.get("budget_frac"), "offered_rps": r(x.get("offered_rps"), 1),

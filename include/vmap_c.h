@@ -55,6 +55,8 @@ typedef enum vmap_status {
 #define VMAP_FLAG_RANGE 4u
 #define VMAP_FLAG_BUFFER_FULL 8u
 #define VMAP_FLAG_BAD_SNAPSHOT 16u /* a loaded snapshot held an invalid or repeated block key */
+#define VMAP_FLAG_STEP_STALLED 32u /* a persistent batch step saw no progress for 2 s and stopped: that step's
+                                     * maps and outputs are incomplete */
 
 /* Voxel storage formats. REF is the reference's Voxel (int16 TSDF x32767,
  * uint8 weight, map_struct.h:17-21); F32 is the plain single-precision map;
@@ -277,6 +279,14 @@ typedef struct vmap_launch_config {
      * changes. */
     int raycast_tile_width;
     int raycast_threads_per_cta;
+    /* how vmap_batch_step runs a batch: 1 = one launch per stage (six, replayed
+     * as a CUDA graph); 2 = one persistent launch whose warps take the items of
+     * every map's stages from a device-side queue, each map's next stage
+     * opening as soon as its previous one finishes; 0 = the default (1). Only
+     * the time changes. Single maps always use the stage launches; the
+     * persistent launch uses raycast_ctas_per_sm for its grid and 256 threads
+     * per CTA. */
+    int batch_schedule;
 } vmap_launch_config;
 vmap_status vmap_get_launch_config(const vmap_map* map, vmap_launch_config* out);
 vmap_status vmap_set_launch_config(vmap_map* map, const vmap_launch_config* cfg);

@@ -31,6 +31,7 @@ def test_candidates_are_valid_launch_values():
         if f.endswith("_ctas_per_sm"):  # grids: 0 (default) .. 64 CTAs per SM
             assert all(0 <= c <= 64 for c in AT.CANDIDATES[f]), f
     assert set(AT.CANDIDATES["raycast_tile_order"]) == {0, 1, 2}
-    assert set(AT.STAGE) | {"mesh_ctas_per_sm"} | set(AT.RAYCAST_PARAMS) == set(AT.FIELDS)
+    assert set(AT.STAGE) | {"mesh_ctas_per_sm", "batch_schedule"} | set(AT.RAYCAST_PARAMS) == set(AT.FIELDS)
+    assert set(AT.CANDIDATES["batch_schedule"]) == {1, 2}
     assert set(AT.CANDIDATES["raycast_tile_width"]) == {4, 8, 16}
     assert set(AT.CANDIDATES["raycast_threads_per_cta"]) == {128, 256}

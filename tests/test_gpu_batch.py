@@ -1,8 +1,9 @@
 """Batched fuse + raycast (vmap_batch_*): a batch step over maps of different
 image sizes, cameras, voxel sizes and pools must leave every map, vertex map
-and normal map bit-identical to driving each map on its own. Steps run on a
-side stream so the graph recording (steps 1-2) and replay (steps 3+) are both
-covered."""
+and normal map bit-identical to driving each map on its own, under both
+schedules (batch_schedule 1: one launch per stage; 2: one persistent launch
+fed by a device-side task queue). Steps run on a side stream so the graph
+recording (steps 1-2) and replay (steps 3+) are both covered."""
 import dataclasses
 
 import numpy as np
@@ -36,12 +37,17 @@ def make_map(wl):
     return vm
 
 
-def test_batch_step_equals_single_map_calls():
+SCHEDULES = pytest.mark.parametrize("schedule", [1, 2], ids=["stages", "persistent"])
+
+
+@SCHEDULES
+def test_batch_step_equals_single_map_calls(schedule):
     wls = workloads()
     scenes = [synth.Scene(wl) for wl in wls]
     batch_maps = [make_map(wl) for wl in wls]
     solo_maps = [make_map(wl) for wl in wls]
     batch = MapBatch(batch_maps)
+    batch.set_launch_config(batch_schedule=schedule)
     side = torch.cuda.Stream()
     for step in range(5):
         depths, rgbs, poses, vb, nb = [], [], [], [], []
@@ -88,7 +94,8 @@ def test_batch_rejects_mixed_formats_and_duplicates():
         MapBatch([a, a])
 
 
-def test_batch_fuse_only_and_render_only_frames():
+@SCHEDULES
+def test_batch_fuse_only_and_render_only_frames(schedule):
     """A step may fuse some maps, render others and leave the rest idle: the
     result equals the matching single-map calls, and idle maps keep their
     visible count."""
@@ -97,6 +104,7 @@ def test_batch_fuse_only_and_render_only_frames():
     batch_maps = [make_map(wl) for wl in wls]
     solo_maps = [make_map(wl) for wl in wls]
     batch = MapBatch(batch_maps)
+    batch.set_launch_config(batch_schedule=schedule)
     side = torch.cuda.Stream()
     # (fuse, render) per map and step; step 0 fuses everything so renders see surface
     plan = [[(1, 1), (1, 1), (1, 1)], [(1, 0), (0, 1), (0, 0)], [(0, 1), (1, 0), (1, 1)],
@@ -141,7 +149,8 @@ def test_batch_fuse_only_and_render_only_frames():
     batch.release()
 
 
-def test_uneven_batch_equals_single_map_calls():
+@SCHEDULES
+def test_uneven_batch_equals_single_map_calls(schedule):
     """Maps of uneven extent, voxel size (4-16 mm), resolution (up to
     1280x720) and pool size in one batch."""
     # pools 4x the generator's so no allocation is refused (which blocks a full
@@ -155,6 +164,7 @@ def test_uneven_batch_equals_single_map_calls():
     for m, wl in zip(batch_maps + solo_maps, wls + wls):
         m.CreateMap(wl.num_entries, wl.num_blocks, wl.voxel_size)
     batch = MapBatch(batch_maps)
+    batch.set_launch_config(batch_schedule=schedule)
     side = torch.cuda.Stream()
     for step in range(3):
         frames = [sc.render(step * 7) for sc in scenes]
@@ -185,7 +195,8 @@ def test_uneven_batch_equals_single_map_calls():
     batch.release()
 
 
-def test_slot_batch_with_maps_in_caller_memory():
+@SCHEDULES
+def test_slot_batch_with_maps_in_caller_memory(schedule):
     """vmap_batch_create_slots + vmap_batch_set_map with maps built by
     vmap_create_in: maps move between slots and sit out steps (empty slot)
     while the recorded graphs are replayed; results equal single-map calls."""
@@ -208,6 +219,10 @@ def test_slot_batch_with_maps_in_caller_memory():
             1 << 18, wls[0].num_blocks, wls[0].voxel_size, torch.empty(1000, dtype=torch.uint8, device="cuda"))
     h = C.c_void_p()
     L.check(lib.vmap_batch_create_slots(5, L.VOXEL_F16, C.byref(h)))
+    cfg = L.LaunchConfig()
+    L.check(lib.vmap_batch_get_launch_config(h, C.byref(cfg)))
+    cfg.batch_schedule = schedule
+    L.check(lib.vmap_batch_set_launch_config(h, C.byref(cfg)))
     f32 = VoxelMapping(64, 48, wls[0].K, voxel_format="f32")
     f32.CreateMap(1 << 10, 1 << 10, 0.01)
     assert lib.vmap_batch_set_map(h, 0, f32._map) == 1
@@ -315,3 +330,63 @@ def test_set_map_on_a_regular_batch_records_again_and_matches_single_calls():
     # the same map in two slots is refused
     assert L.lib().vmap_batch_set_map(batch._h, 0, c._map) == 1
     batch.release()
+
+
+def test_persistent_step_equals_stage_launches_on_many_maps():
+    """40 maps (more than the task ring's first wave of openers needs), small
+    and full-size images, one rendered in raycast mode 1, two left idle in
+    some steps: the persistent step and the stage launches give bit-identical
+    vertex maps, normal maps and voxels."""
+    base = synth.WORKLOADS["room_small"]
+    wls = [dataclasses.replace(base, seed=100 + i, width=96 + 8 * (i % 5), height=64 + 4 * (i % 3),
+                               fx=90.0 + i, fy=90.0 + i, cx=48.0 + 4 * (i % 5), cy=32.0 + 2 * (i % 3),
+                               voxel_format="f16", num_blocks=1 << 13, with_color=i % 2 == 0) for i in range(38)]
+    wls += [dataclasses.replace(synth.WORKLOADS["room_full"], seed=200 + i, voxel_format="f16", num_blocks=1 << 16,
+                                with_color=True) for i in range(2)]
+    scenes = [synth.Scene(wl) for wl in wls]
+
+    def mk(i, wl):
+        vm = VoxelMapping(wl.width, wl.height, wl.K, voxel_format="f16", with_color=wl.with_color, max_weight=128,
+                          raycast_mode=1 if i == 7 else 0)
+        vm.CreateMap(1 << 15 if wl.num_blocks < (1 << 16) else 1 << 18, wl.num_blocks, wl.voxel_size)
+        return vm
+
+    maps = {s: [mk(i, wl) for i, wl in enumerate(wls)] for s in (1, 2)}
+    batches = {s: MapBatch(maps[s]) for s in (1, 2)}
+    for s, b in batches.items():
+        b.set_launch_config(batch_schedule=s)
+    side = torch.cuda.Stream()
+    for step in range(4):
+        fr = [sc.render(step * 5) for sc in scenes]
+        idle = {3, 11} if step % 2 else set()
+        depths = [None if i in idle else torch.from_numpy(d.view(np.int16)).cuda() for i, (d, _, _) in enumerate(fr)]
+        rgbs = [torch.from_numpy(c).cuda().reshape(wl.height, -1) if wl.with_color and i not in idle else None
+                for i, ((_, c, _), wl) in enumerate(zip(fr, wls))]
+        poses = [p for _, _, p in fr]
+        outs = {}
+        for s, b in batches.items():
+            vb = [None if i in idle else torch.full((wl.height, wl.width, 4), 7.0, device="cuda")
+                  for i, wl in enumerate(wls)]
+            nb = [None if v is None else torch.full_like(v, 7.0) for v in vb]
+            torch.cuda.synchronize()
+            with torch.cuda.stream(side):
+                b.step(depths, rgbs, poses, vb, nb)
+            side.synchronize()
+            outs[s] = (vb, nb)
+        for i in range(len(wls)):
+            if i in idle:
+                continue
+            for k in (0, 1):
+                a, c = outs[1][k][i].cpu().numpy(), outs[2][k][i].cpu().numpy()
+                assert np.array_equal(np.nan_to_num(a, nan=-9.0), np.nan_to_num(c, nan=-9.0)), (step, i, k)
+    hit = np.mean([np.isfinite(v.cpu().numpy()[..., 0]).mean() for v in outs[2][0] if v is not None])
+    assert hit > 0.3
+    for i, (a, c) in enumerate(zip(maps[1], maps[2])):
+        ea, ec = a.export_blocks(), c.export_blocks()
+        ia, ic = np.argsort(block_keys(ea["coords"])), np.argsort(block_keys(ec["coords"]))
+        for k in ("coords", "tsdf", "weight") + (("rgb",) if wls[i].with_color else ()):
+            assert np.array_equal(ea[k][ia], ec[k][ic]), (i, k)
+        assert a.stats()["visible_blocks"] == c.stats()["visible_blocks"], i
+        assert a.stats()["error_flags"] == c.stats()["error_flags"] == 0, i
+    for b in batches.values():
+        b.release()

@@ -1,8 +1,9 @@
-"""Kernel resources as ptxas reports them (no GPU): the ray marcher fits the
-64 registers that 4 resident CTAs of 256 threads per SM leave it
-(__launch_bounds__(256, 4)) with a small spill, the other kernels spill at
-most a few words, and no kernel needs more static shared memory than the
-48 KB a launch gets without opting in."""
+"""Kernel resources as ptxas reports them (no GPU): the ray marcher and the
+persistent batch step (which contains it) fit the 64 registers that 4
+resident CTAs of 256 threads per SM leave them (__launch_bounds__(256, 4))
+with a small spill, the other kernels spill at most a few words, and no
+kernel needs more static shared memory than the 48 KB a launch gets without
+opting in."""
 import pytest
 
 from voxelmapping_b200 import build as B
@@ -30,8 +31,15 @@ def test_ray_marcher_fits_four_ctas_per_sm(report):
         assert r["registers"] <= 64 and r["spill_stores"] <= 320, (k, r)
 
 
+def test_persistent_step_fits_four_ctas_per_sm(report):
+    st = {k: r for k, r in report.items() if "step_kernel" in k}
+    assert len(st) == 4  # four voxel formats
+    for k, r in st.items():
+        assert r["registers"] <= 64 and r["spill_stores"] <= 320 and 4 * r["smem"] <= 227 * 1024, (k, r)
+
+
 def test_other_kernels_barely_spill_and_fit_default_shared_memory(report):
     for k, r in report.items():
-        if "raycast_kernel" not in k:
+        if "raycast_kernel" not in k and "step_kernel" not in k:
             assert r["spill_stores"] <= 32, (k, r)
         assert r["smem"] <= 48 * 1024, (k, r)

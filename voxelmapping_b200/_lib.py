@@ -15,7 +15,7 @@ STATUS_NAMES = {0: "VMAP_OK", 1: "VMAP_ERR_INVALID_ARG", 2: "VMAP_ERR_CUDA", 3: 
                 4: "VMAP_ERR_POOL_FULL", 5: "VMAP_ERR_HASH_FULL", 6: "VMAP_ERR_RANGE",
                 7: "VMAP_ERR_BUFFER_FULL", 8: "VMAP_ERR_NO_DEVICE"}
 
-FLAG_POOL_FULL, FLAG_HASH_FULL, FLAG_RANGE, FLAG_BUFFER_FULL, FLAG_BAD_SNAPSHOT = 1, 2, 4, 8, 16
+FLAG_POOL_FULL, FLAG_HASH_FULL, FLAG_RANGE, FLAG_BUFFER_FULL, FLAG_BAD_SNAPSHOT, FLAG_STEP_STALLED = 1, 2, 4, 8, 16, 32
 
 VOXEL_REF, VOXEL_F32, VOXEL_F16, VOXEL_I16 = 0, 1, 2, 3
 FORMAT_NAMES = {"ref": VOXEL_REF, "f32": VOXEL_F32, "f16": VOXEL_F16, "i16": VOXEL_I16}
@@ -65,7 +65,8 @@ class LaunchConfig(C.Structure):
     _fields_ = [("alloc_ctas_per_sm", C.c_int), ("visibility_ctas_per_sm", C.c_int), ("fuse_ctas_per_sm", C.c_int),
                 ("zrange_ctas_per_sm", C.c_int), ("raycast_ctas_per_sm", C.c_int), ("normals_ctas_per_sm", C.c_int),
                 ("mesh_ctas_per_sm", C.c_int), ("raycast_tile_order", C.c_int),
-                ("raycast_tile_width", C.c_int), ("raycast_threads_per_cta", C.c_int)]
+                ("raycast_tile_width", C.c_int), ("raycast_threads_per_cta", C.c_int),
+                ("batch_schedule", C.c_int)]
 
 
 class SnapshotHeader(C.Structure):

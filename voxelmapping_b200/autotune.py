@@ -30,7 +30,7 @@ from . import _lib as L
 
 FIELDS = ["alloc_ctas_per_sm", "visibility_ctas_per_sm", "fuse_ctas_per_sm", "zrange_ctas_per_sm",
           "raycast_ctas_per_sm", "normals_ctas_per_sm", "mesh_ctas_per_sm", "raycast_tile_order",
-          "raycast_tile_width", "raycast_threads_per_cta"]
+          "raycast_tile_width", "raycast_threads_per_cta", "batch_schedule"]
 # the ray marcher's parameters besides its grid, swept one at a time
 RAYCAST_PARAMS = ["raycast_tile_width", "raycast_threads_per_cta", "raycast_tile_order"]
 STAGE = {"alloc_ctas_per_sm": "alloc", "visibility_ctas_per_sm": "visibility", "fuse_ctas_per_sm": "fuse",
@@ -46,6 +46,7 @@ CANDIDATES = {
     "raycast_tile_order": [0, 1, 2],  # bottom rows first, top rows first, alternating ends
     "raycast_tile_width": [8, 16, 4],  # 8x4, 16x2 or 4x8 rays per warp
     "raycast_threads_per_cta": [256, 128],
+    "batch_schedule": [2, 1],  # one persistent launch per batch step, or one launch per stage
 }
 SHIPPED = Path(__file__).resolve().parent / "tuning_b200.json"
 
@@ -194,7 +195,8 @@ def tune_batch(batch, step, n_steps=4, rounds=2, fields=None):
     best = batch.get_launch_config()
     table = {}
     it = 0
-    for f in fields or [f for f in FIELDS if f != "mesh_ctas_per_sm"]:
+    # the schedule first: the persistent launch has one grid (raycast_ctas_per_sm)
+    for f in fields or ["batch_schedule"] + [f for f in FIELDS if f not in ("mesh_ctas_per_sm", "batch_schedule")]:
         samples = {c: [] for c in CANDIDATES[f]}
         for _ in range(rounds):
             for c in samples:

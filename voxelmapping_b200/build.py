@@ -20,8 +20,8 @@ OBJ = PKG / "_build"
 LIB = PKG / "libvmap_b200.so"
 SYNTH = PKG / "libvmap_synth.so"
 
-CUDA_SOURCES = ["fusion.cu", "raycast.cu", "raymarch.cu", "mesh.cu", "map.cu", "batch.cu", "export_static.cu", "snapshot.cu",
-                "vmapping.cpp"]
+CUDA_SOURCES = ["fusion.cu", "raycast.cu", "raymarch.cu", "step.cu", "mesh.cu", "map.cu", "batch.cu", "export_static.cu",
+                "snapshot.cu", "vmapping.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-ffp-contract=off,-Wall",
                      "--expt-relaxed-constexpr", "-I" + str(ROOT / "include")]
@@ -80,8 +80,8 @@ def build(verbose=False):
     return LIB
 
 
-def ptxas_report(sources=("raymarch.cu", "fusion.cu", "mesh.cu", "raycast.cu", "batch.cu", "export_static.cu",
-                           "snapshot.cu", "map.cu")):
+def ptxas_report(sources=("raymarch.cu", "step.cu", "fusion.cu", "mesh.cu", "raycast.cu", "batch.cu",
+                           "export_static.cu", "snapshot.cu", "map.cu")):
     """Per-kernel resources as ptxas reports them (-Xptxas -v) for the given
     CUDA sources, compiled with the library's flags into a temporary
     directory: {kernel (demangled): {"registers", "spill_stores",

@@ -17,7 +17,7 @@
 #include <new>
 #include <vector>
 
-#include "vmap_launch.h"
+#include "step.h"
 
 using namespace vmapb;
 
@@ -35,6 +35,7 @@ struct vmap_batch {
     MapView* dViews[2];      // device descriptors, one set per buffer
     MapView* hViews[2];      // pinned staging
     unsigned* dQueue;        // raycast work queue
+    StepSched* dSched;       // scheduler of the persistent step
     cudaEvent_t copied[2];   // the copy out of staging b has executed
     bool eventUsed[2];
     cudaGraphExec_t exec[2];
@@ -65,6 +66,7 @@ void release(vmap_batch* b)
         if (b->hViews[i]) cudaFreeHost(b->hViews[i]);
     }
     cudaFree(b->dQueue);
+    cudaFree(b->dSched);
 }
 
 // Work-item count that makes the alloc and normals launches use their full
@@ -85,6 +87,7 @@ vmap_status finish_create(vmap_batch* b, vmap_batch** out)
         if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->copied[i], cudaEventDisableTiming);
     }
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->dQueue, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->dSched, sizeof(StepSched));
     if (e != cudaSuccess) {
         vmap_status st = fail(e, "vmap_batch_create");
         release(b);
@@ -95,10 +98,12 @@ vmap_status finish_create(vmap_batch* b, vmap_batch** out)
     return VMAP_OK;
 }
 
-// The six stage launches of one step over the descriptors in dViews[buf].
+// One step over the descriptors in dViews[buf]: the persistent launch, or
+// the six stage launches.
 cudaError_t enqueue_stages(vmap_batch* b, int buf, cudaStream_t s)
 {
     ManyViews mv{b->dViews[buf], (int)b->maps.size(), b->dQueue};
+    if (b->launcher.batchSchedule == 2) return launch_step(mv, b->dSched, b->fmt, b->launcher, s);
     cudaError_t e;
     if ((e = launch_alloc(mv, b->totalAllocTiles, b->launcher, s)) != cudaSuccess) return e;
     if ((e = launch_visibility(mv, b->launcher, s)) != cudaSuccess) return e;

@@ -196,6 +196,19 @@ __device__ __forceinline__ bool block_visible(int bx, int by, int bz, const Xf& 
     return false;
 }
 
+// ------------------------------------------------------------- map loads
+// Stage kernels read map data that no thread writes while the kernel runs
+// (hash slots, voxels, links, tile bounds, vertex maps) through the read-only
+// path (NC = true). The persistent batch step writes such data in one stage
+// and reads it in a later one of the same launch, so it reads with plain
+// loads (NC = false), ordered after the acquire that opened the stage.
+template <bool NC, class T>
+__device__ __forceinline__ T ld_map(const T* p)
+{
+    if constexpr (NC) return __ldg(p);
+    else return *p;
+}
+
 // ------------------------------------------------------------- hash table
 // Bucketed open hashing: bucket = reference hash of the block coordinates,
 // 4 slots per bucket (key and pool slot side by side: one 64-byte read per
@@ -203,6 +216,7 @@ __device__ __forceinline__ bool block_visible(int bx, int by, int bz, const Xf& 
 // bucket when all 4 are taken. Slots go EMPTY -> key exactly once, so the
 // filled slots of a bucket always form a prefix: a lookup stops at the first
 // EMPTY slot.
+template <bool NC = true>
 __device__ __forceinline__ int hash_find(const DevMap& m, int bx, int by, int bz)
 {
     if (!coord_ok(bx, by, bz)) return -1;
@@ -211,7 +225,7 @@ __device__ __forceinline__ int hash_find(const DevMap& m, int bx, int by, int bz
 #pragma unroll 1
     for (int p = 0; p < kMaxProbe; ++p) {
         const ulonglong2* s = m.slots + (size_t)b * kSlots;
-        const ulonglong2 a0 = __ldg(s), a1 = __ldg(s + 1), a2 = __ldg(s + 2), a3 = __ldg(s + 3);
+        const ulonglong2 a0 = ld_map<NC>(s), a1 = ld_map<NC>(s + 1), a2 = ld_map<NC>(s + 2), a3 = ld_map<NC>(s + 3);
         if (a0.x == key) return (int)a0.y;
         if (a0.x == kEmptyKey) return -1;
         if (a1.x == key) return (int)a1.y;

@@ -27,6 +27,7 @@ struct Launcher {
     int tileOrder = 0;  // ray-marcher tile order (vmap_launch_config.raycast_tile_order)
     int tileW = 8;       // ray-marcher tile width; the tile is 32 rays
     int rayThreads = 256;  // ray-marcher threads per CTA
+    int batchSchedule = 1;  // vmap_launch_config.batch_schedule
 };
 
 // vmap_launch_config <-> Launcher (0 in a field: the default)
@@ -38,7 +39,7 @@ inline bool launch_config_ok(const vmap_launch_config* c)
         if (x < 0 || x > 64) return false;
     const int tw = c->raycast_tile_width, tt = c->raycast_threads_per_cta;
     return c->raycast_tile_order >= 0 && c->raycast_tile_order <= 2 && (tw == 0 || tw == 4 || tw == 8 || tw == 16) &&
-           (tt == 0 || tt == 128 || tt == 256);
+           (tt == 0 || tt == 128 || tt == 256) && c->batch_schedule >= 0 && c->batch_schedule <= 2;
 }
 
 inline void launch_config_to(const vmap_launch_config* c, Launcher& l)
@@ -54,6 +55,7 @@ inline void launch_config_to(const vmap_launch_config* c, Launcher& l)
     l.tileOrder = c->raycast_tile_order;
     l.tileW = c->raycast_tile_width ? c->raycast_tile_width : d.tileW;
     l.rayThreads = c->raycast_threads_per_cta ? c->raycast_threads_per_cta : d.rayThreads;
+    l.batchSchedule = c->batch_schedule ? c->batch_schedule : d.batchSchedule;
 }
 
 inline void launch_config_from(const Launcher& l, vmap_launch_config* c)
@@ -68,6 +70,7 @@ inline void launch_config_from(const Launcher& l, vmap_launch_config* c)
     c->raycast_tile_order = l.tileOrder;
     c->raycast_tile_width = l.tileW;
     c->raycast_threads_per_cta = l.rayThreads;
+    c->batch_schedule = l.batchSchedule;
 }
 
 // grid of `per_sm` CTAs per SM, or fewer when there are fewer work items
