@@ -1,7 +1,8 @@
 """Kernel resources as ptxas reports them (no GPU): the ray marcher and the
 persistent batch step (which contains it) fit the 64 registers that 4
 resident CTAs of 256 threads per SM leave them (__launch_bounds__(256, 4))
-with a small spill, the other kernels spill at most a few words, and no
+with a small spill, fusion and allocation keep their occupancy caps with at
+most 64 B of spill, the other kernels spill at most a few words, and no
 kernel needs more static shared memory than the 48 KB a launch gets without
 opting in."""
 import pytest
@@ -40,6 +41,9 @@ def test_persistent_step_fits_four_ctas_per_sm(report):
 
 def test_other_kernels_barely_spill_and_fit_default_shared_memory(report):
     for k, r in report.items():
-        if "raycast_kernel" not in k and "step_kernel" not in k:
+        if "fuse_kernel" in k or "alloc_kernel" in k:
+            # occupancy caps (6 and 8 CTAs per SM), measured faster with this small spill
+            assert r["registers"] <= (40 if "fuse_kernel" in k else 32) and r["spill_stores"] <= 64, (k, r)
+        elif "raycast_kernel" not in k and "step_kernel" not in k:
             assert r["spill_stores"] <= 32, (k, r)
         assert r["smem"] <= 48 * 1024, (k, r)

@@ -167,12 +167,14 @@ __device__ __forceinline__ void visibility_group(const MapView& v, int g, int la
 }
 
 // ----------------------------------------------------------------- fusion
-// DepthFusionFunctor / ImageFusionFunctor for the 4 consecutive voxels
-// v0 .. v0 + 3 of an x-row of block `slot` (one 16- or 32-byte vector of
-// voxel words, one 4-byte word per colour plane). The voxel words are loaded
-// before the projections so the load overlaps the arithmetic; nothing is
-// written unless one of the 4 voxels updates.
-template <int FMT, bool COLOR, int DT>
+// DepthFusionFunctor / ImageFusionFunctor for the NV (4 or 8) consecutive
+// voxels v0 .. v0 + NV - 1 of an x-row of block `slot` (one vector of NV
+// voxel words, one NV-byte word per colour plane). Every load is issued as
+// early as its address is known, so a thread waits on two memory round trips
+// rather than four: the voxel words and colour planes before the projections,
+// each projected pixel's depth and colour right after its projection. Nothing
+// is written unless one of the 4 voxels updates.
+template <int FMT, bool COLOR, int DT, int NV = 4>
 __device__ __forceinline__ void fuse_block(const MapView& v, int slot, int v0)
 {
     typedef Layout<FMT> L;
@@ -182,25 +184,35 @@ __device__ __forceinline__ void fuse_block(const MapView& v, int slot, int v0)
     const int lx0 = v0 & 7, ly = (v0 >> 3) & 7, lz = v0 >> 6;
     const int3 bp = unpack_key(m.blockKeys[slot]);
     Word* blk = L::words_rw(m, slot);
-    Word w[4];
-    load_vec<4 * sizeof(Word)>(blk + v0, w);
+    static_assert(NV == 4 || NV == 8, "4 or 8 voxels of an x-row");
+    Word w[NV];
+    load_vec<NV * sizeof(Word)>(blk + v0, w);
+    unsigned char c[3][NV];
+    unsigned char* crow = reinterpret_cast<unsigned char*>(blk) + L::kRgbOff + v0;
+    if constexpr (COLOR) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) load_vec<NV>(crow + k * kBlockVoxels, c[k]);
+    }
     const int vx0 = bp.x * 8 + lx0;
     const float wy = __fmul_rn(__int2float_rn(bp.y * 8 + ly), m.vs);
     const float wz = __fmul_rn(__int2float_rn(bp.z * 8 + lz), m.vs);
-    float sdfv[4];
-    int pu[4], pv[4];
+    float sdfv[NV];
+    unsigned pix[NV];  // the projected pixel's colour, r | g << 8 | b << 16
     unsigned mask = 0;
 #pragma unroll
-    for (int x = 0; x < 4; ++x) {
+    for (int x = 0; x < NV; ++x) {
         const float3 p = xf_apply(v.Ti, __fmul_rn(__int2float_rn(vx0 + x), m.vs), wy, wz);
         // __float2int_rd(fx * p0 / p2 + cx + 0.5)
         const int u = __float2int_rd(__fadd_rn(__fadd_rn(__fdiv_rn(__fmul_rn(v.cam.fx, p.x), p.z), v.cam.cx), 0.5f));
         const int vv = __float2int_rd(__fadd_rn(__fadd_rn(__fdiv_rn(__fmul_rn(v.cam.fy, p.y), p.z), v.cam.cy), 0.5f));
-        pu[x] = u;
-        pv[x] = vv;
         sdfv[x] = 0.f;
+        pix[x] = 0u;
         if (u < 0 || vv < 0 || u > v.cam.W - 1 || vv > v.cam.H - 1) continue;
         const float d = read_depth_t<DT>(v.in, u, vv);
+        if constexpr (COLOR) {
+            const uint8_t* px = v.in.rgb + (size_t)vv * v.in.rgbPitch + 3 * u;
+            pix[x] = (unsigned)__ldg(px) | ((unsigned)__ldg(px + 1) << 8) | ((unsigned)__ldg(px + 2) << 16);
+        }
         if (isnan(d) || d > kMaxDepth || d < kMinDepth) continue;
         const float sdf = __fsub_rn(d, p.z);
         if (sdf < -m.mu) continue;
@@ -208,23 +220,15 @@ __device__ __forceinline__ void fuse_block(const MapView& v, int slot, int v0)
         mask |= 1u << x;
     }
     if (!mask) return;
-    unsigned char c[3][4];
-    unsigned char* crow = reinterpret_cast<unsigned char*>(blk) + L::kRgbOff + v0;
-    if constexpr (COLOR) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) load_vec<4>(crow + k * kBlockVoxels, c[k]);
-    }
-#pragma unroll
-    for (int x = 0; x < 4; ++x) {
+    for (int x = 0; x < NV; ++x) {
         if (!(mask & (1u << x))) continue;
         const float ow = F::weight(w[x]);
-        const uint8_t* px = nullptr;
-        if constexpr (COLOR) px = v.in.rgb + (size_t)pv[x] * v.in.rgbPitch + 3 * pu[x];
         if (ow == 0.f) {
             w[x] = F::make(sdfv[x], 1.f);
             if constexpr (COLOR) {
 #pragma unroll
-                for (int k = 0; k < 3; ++k) c[k][x] = __ldg(px + k);
+                for (int k = 0; k < 3; ++k) c[k][x] = (unsigned char)(pix[x] >> (8 * k));
             }
         } else {
             const float os = F::tsdf(w[x]);
@@ -232,30 +236,30 @@ __device__ __forceinline__ void fuse_block(const MapView& v, int slot, int v0)
             if constexpr (COLOR) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k)
-                    c[k][x] = (unsigned char)__float2int_rz(
-                        __fmaf_rn(0.7f, __uint2float_rn(c[k][x]), __fmul_rn(0.3f, __uint2float_rn(__ldg(px + k)))));
+                    c[k][x] = (unsigned char)__float2int_rz(__fmaf_rn(
+                        0.7f, __uint2float_rn(c[k][x]), __fmul_rn(0.3f, __uint2float_rn((pix[x] >> (8 * k)) & 0xffu))));
             }
         }
     }
-    store_vec<4 * sizeof(Word)>(blk + v0, w);
+    store_vec<NV * sizeof(Word)>(blk + v0, w);
     if constexpr (COLOR) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) store_vec<4>(crow + k * kBlockVoxels, c[k]);
+        for (int k = 0; k < 3; ++k) store_vec<NV>(crow + k * kBlockVoxels, c[k]);
     }
 }
 
 // fuse_block for the frame's depth type; colour when the frame carries it
 // (the map must keep colour).
-template <int FMT>
+template <int FMT, int NV = 4>
 __device__ __forceinline__ void fuse_voxels(const MapView& v, int slot, int v0)
 {
     const bool color = v.in.rgb != nullptr;
     if (v.in.dtype == VMAP_DEPTH_U16) {
-        if (color) fuse_block<FMT, true, VMAP_DEPTH_U16>(v, slot, v0);
-        else fuse_block<FMT, false, VMAP_DEPTH_U16>(v, slot, v0);
+        if (color) fuse_block<FMT, true, VMAP_DEPTH_U16, NV>(v, slot, v0);
+        else fuse_block<FMT, false, VMAP_DEPTH_U16, NV>(v, slot, v0);
     } else {
-        if (color) fuse_block<FMT, true, VMAP_DEPTH_F32>(v, slot, v0);
-        else fuse_block<FMT, false, VMAP_DEPTH_F32>(v, slot, v0);
+        if (color) fuse_block<FMT, true, VMAP_DEPTH_F32, NV>(v, slot, v0);
+        else fuse_block<FMT, false, VMAP_DEPTH_F32, NV>(v, slot, v0);
     }
 }
 
