@@ -26,30 +26,27 @@
 namespace vmapb {
 
 // ------------------------------------------------------------------ z-range
-// One thread per task: first the neighbour links of the blocks allocated
-// since the last pass, [ctr[C_LINKED], allocated) (in both raycast modes:
-// the ray marcher, which always follows, reads the links for trilinear
-// corners in neighbouring blocks and advances C_LINKED), then one z-range
-// fold per allocated block of the maps rendered in mode 0. Block 0 also
+// One thread per task, in one index space per map: first the neighbour links
+// of the blocks allocated since the last pass, [ctr[C_LINKED], allocated) (in
+// both raycast modes: the ray marcher, which always follows, reads the links
+// for trilinear corners in neighbouring blocks and advances C_LINKED), then
+// one z-range fold per allocated block of the maps rendered in mode 0. The
+// two kinds of task are independent, so they share one pass. Block 0 also
 // rewinds the raycast work queue for the kernel that follows.
 template <class V>
 __global__ void __launch_bounds__(256) zrange_kernel(V views)
 {
     __shared__ int pre[kMaxBatch + 1];
     const int nmaps = views.count();
-    map_prefix(views, [](const MapView& v) { return links_pending(v); }, pre);
-    const int ntasks = pre[nmaps];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < ntasks; i += gridDim.x * blockDim.x) {
-        const int mi = map_of(pre, nmaps, i);
-        link_task<true>(views[mi].m, i - pre[mi]);
-    }
-    __syncthreads();  // `pre` is reused
-    map_prefix(views, [](const MapView& v) { return zrange_blocks(v); }, pre);
+    map_prefix(views, [](const MapView& v) { return links_pending(v) + zrange_blocks(v); }, pre);
     if (blockIdx.x == 0 && threadIdx.x == 0) views.queue[0] = 0u;
     const int total = pre[nmaps];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
         const int mi = map_of(pre, nmaps, i);
-        zrange_block(views[mi], i - pre[mi]);
+        const MapView& v = views[mi];
+        const int t = i - pre[mi], nlink = links_pending(v);
+        if (t < nlink) link_task<true>(v.m, t);
+        else zrange_block(v, t - nlink);
     }
 }
 

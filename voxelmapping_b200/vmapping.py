@@ -339,8 +339,10 @@ class MapBatch:
 
     step(depths, rgbs, poses, vmaps, nmaps) fuses depths[i] (and rgbs[i]) into
     maps[i] at poses[i] and raycasts maps[i] at the same pose into vmaps[i]
-    (and nmaps[i]); every stage is one launch over all maps, replayed as a CUDA
-    graph from the third step on (non-default streams)."""
+    (and nmaps[i]). By default every stage is one launch over all maps;
+    set_launch_config(batch_schedule=2) runs the whole step as one persistent
+    launch instead (same results). Either is replayed as a CUDA graph from the
+    third step on (non-default streams)."""
 
     def __init__(self, maps):
         self.maps = list(maps)
