@@ -27,6 +27,7 @@ constexpr int kTileSet = 1024;  // open-addressed set of one tile's blocks (8 KB
 template <class V>
 __global__ void __launch_bounds__(256, 8) alloc_kernel(V views)
 {
+    stage_entry();
     __shared__ int pre[kMaxBatch + 1];
     __shared__ unsigned long long set[kTileSet];
     for (int i = threadIdx.x; i < kTileSet; i += blockDim.x) set[i] = kEmptyKey;
@@ -63,6 +64,7 @@ __global__ void __launch_bounds__(256, 8) alloc_kernel(V views)
 template <class V>
 __global__ void __launch_bounds__(256) visibility_kernel(V views)
 {
+    stage_entry();
     __shared__ int pre[kMaxBatch + 1];
     map_prefix(views, [](const MapView& v) { return v.in.active ? (allocated_blocks(v.m) + 31) >> 5 : 0; }, pre);
     const int nmaps = views.count();
@@ -87,6 +89,7 @@ constexpr int kFuseTeam = kBlockVoxels / kFuseVoxels;
 template <class V, int FMT>
 __global__ void __launch_bounds__(256, 6) fuse_kernel(V views)
 {
+    stage_entry();
     __shared__ int pre[kMaxBatch + 1];
     map_prefix(views, [](const MapView& v) { return v.in.active ? (int)v.m.ctr[C_VISIBLE] : 0; }, pre);
     const int nmaps = views.count();
@@ -116,15 +119,13 @@ __global__ void reset_hash_kernel(DevMap m)
 template <class V>
 cudaError_t launch_alloc(const V& views, int totalTiles, const Launcher& l, cudaStream_t s)
 {
-    alloc_kernel<V><<<stage_grid(l, l.alloc, totalTiles), 256, 0, s>>>(views);
-    return cudaGetLastError();
+    return launch_stage(alloc_kernel<V>, stage_grid(l, l.alloc, totalTiles), 256, s, views);
 }
 
 template <class V>
 cudaError_t launch_visibility(const V& views, const Launcher& l, cudaStream_t s)
 {
-    visibility_kernel<V><<<stage_grid(l, l.visibility), 256, 0, s>>>(views);
-    return cudaGetLastError();
+    return launch_stage(visibility_kernel<V>, stage_grid(l, l.visibility), 256, s, views);
 }
 
 template <class V>
@@ -132,13 +133,12 @@ cudaError_t launch_fuse(const V& views, int fmt, const Launcher& l, cudaStream_t
 {
     const int grid = stage_grid(l, l.fuse);
     switch (fmt) {
-    case VMAP_VOXEL_REF: fuse_kernel<V, VMAP_VOXEL_REF><<<grid, 256, 0, s>>>(views); break;
-    case VMAP_VOXEL_F32: fuse_kernel<V, VMAP_VOXEL_F32><<<grid, 256, 0, s>>>(views); break;
-    case VMAP_VOXEL_F16: fuse_kernel<V, VMAP_VOXEL_F16><<<grid, 256, 0, s>>>(views); break;
-    case VMAP_VOXEL_I16: fuse_kernel<V, VMAP_VOXEL_I16><<<grid, 256, 0, s>>>(views); break;
+    case VMAP_VOXEL_REF: return launch_stage(fuse_kernel<V, VMAP_VOXEL_REF>, grid, 256, s, views);
+    case VMAP_VOXEL_F32: return launch_stage(fuse_kernel<V, VMAP_VOXEL_F32>, grid, 256, s, views);
+    case VMAP_VOXEL_F16: return launch_stage(fuse_kernel<V, VMAP_VOXEL_F16>, grid, 256, s, views);
+    case VMAP_VOXEL_I16: return launch_stage(fuse_kernel<V, VMAP_VOXEL_I16>, grid, 256, s, views);
     default: return cudaErrorInvalidValue;
     }
-    return cudaGetLastError();
 }
 
 template cudaError_t launch_alloc<OneView>(const OneView&, int, const Launcher&, cudaStream_t);

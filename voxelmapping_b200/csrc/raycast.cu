@@ -36,6 +36,7 @@ namespace vmapb {
 template <class V>
 __global__ void __launch_bounds__(256) zrange_kernel(V views)
 {
+    stage_entry();
     __shared__ int pre[kMaxBatch + 1];
     const int nmaps = views.count();
     map_prefix(views, [](const MapView& v) { return links_pending(v) + zrange_blocks(v); }, pre);
@@ -55,6 +56,7 @@ __global__ void __launch_bounds__(256) zrange_kernel(V views)
 template <class V>
 __global__ void __launch_bounds__(256) normals_kernel(V views)
 {
+    stage_entry();
     __shared__ int pre[kMaxBatch + 1];
     map_prefix(views, [](const MapView& v) { return normal_tiles(v); }, pre);
     const int nmaps = views.count();
@@ -103,15 +105,13 @@ __global__ void __launch_bounds__(256) phong_kernel(const float4* vmap, size_t v
 template <class V>
 cudaError_t launch_zrange(const V& views, const Launcher& l, cudaStream_t s)
 {
-    zrange_kernel<V><<<stage_grid(l, l.zrange), 256, 0, s>>>(views);
-    return cudaGetLastError();
+    return launch_stage(zrange_kernel<V>, stage_grid(l, l.zrange), 256, s, views);
 }
 
 template <class V>
 cudaError_t launch_normals(const V& views, int totalTiles, const Launcher& l, cudaStream_t s)
 {
-    normals_kernel<V><<<stage_grid(l, l.normals, totalTiles), 256, 0, s>>>(views);
-    return cudaGetLastError();
+    return launch_stage(normals_kernel<V>, stage_grid(l, l.normals, totalTiles), 256, s, views);
 }
 
 template cudaError_t launch_zrange<OneView>(const OneView&, const Launcher&, cudaStream_t);

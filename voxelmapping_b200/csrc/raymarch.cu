@@ -32,6 +32,7 @@ namespace vmapb {
 template <class V, int FMT>
 __global__ void __launch_bounds__(256, 4) raycast_kernel(const __grid_constant__ V views, int order, int tw)
 {
+    stage_entry();
     __shared__ int pre[kMaxBatch + 1];
     __shared__ unsigned long long s_wkey[8][kWarpCache];
     __shared__ int s_wslot[8][kWarpCache];
@@ -84,8 +85,7 @@ static cudaError_t raycast_persistent(const V& views, const Launcher& l, cudaStr
     const int fit = occ[threads == 256];
     // CTAs beyond those resident would only start once others finish: cap at occupancy
     const int per_sm = l.raycast > 0 && l.raycast < fit ? l.raycast : fit;
-    raycast_kernel<V, FMT><<<stage_grid(l, per_sm), threads, 0, s>>>(views, l.tileOrder, l.tileW);
-    return cudaGetLastError();
+    return launch_stage(raycast_kernel<V, FMT>, stage_grid(l, per_sm), threads, s, views, l.tileOrder, l.tileW);
 }
 
 template <class V>

@@ -9,6 +9,7 @@
 #include <stdint.h>
 
 #include <string>
+#include <utility>
 
 #include "vmap_internal.cuh"
 
@@ -79,6 +80,24 @@ inline int stage_grid(const Launcher& l, int per_sm, long long items = -1)
     const long long g = (long long)l.numSMs * per_sm;
     if (items >= 0 && items < g) return items > 0 ? (int)items : 1;
     return (int)g;
+}
+
+// Launch of a per-frame stage kernel with programmatic stream serialization
+// (the kernel must call stage_entry() first).
+template <typename... KArgs, typename... Args>
+cudaError_t launch_stage(void (*kernel)(KArgs...), int grid, int block, cudaStream_t s, Args&&... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)grid);
+    cfg.blockDim = dim3((unsigned)block);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
 }
 
 // fusion.cu
