@@ -119,13 +119,13 @@ __global__ void reset_hash_kernel(DevMap m)
 template <class V>
 cudaError_t launch_alloc(const V& views, int totalTiles, const Launcher& l, cudaStream_t s)
 {
-    return launch_stage(alloc_kernel<V>, stage_grid(l, l.alloc, totalTiles), 256, s, views);
+    return launch_stage<V>(alloc_kernel<V>, stage_grid(l, l.alloc, totalTiles), 256, s, views);
 }
 
 template <class V>
 cudaError_t launch_visibility(const V& views, const Launcher& l, cudaStream_t s)
 {
-    return launch_stage(visibility_kernel<V>, stage_grid(l, l.visibility), 256, s, views);
+    return launch_stage<V>(visibility_kernel<V>, stage_grid(l, l.visibility), 256, s, views);
 }
 
 template <class V>
@@ -133,10 +133,10 @@ cudaError_t launch_fuse(const V& views, int fmt, const Launcher& l, cudaStream_t
 {
     const int grid = stage_grid(l, l.fuse);
     switch (fmt) {
-    case VMAP_VOXEL_REF: return launch_stage(fuse_kernel<V, VMAP_VOXEL_REF>, grid, 256, s, views);
-    case VMAP_VOXEL_F32: return launch_stage(fuse_kernel<V, VMAP_VOXEL_F32>, grid, 256, s, views);
-    case VMAP_VOXEL_F16: return launch_stage(fuse_kernel<V, VMAP_VOXEL_F16>, grid, 256, s, views);
-    case VMAP_VOXEL_I16: return launch_stage(fuse_kernel<V, VMAP_VOXEL_I16>, grid, 256, s, views);
+    case VMAP_VOXEL_REF: return launch_stage<V>(fuse_kernel<V, VMAP_VOXEL_REF>, grid, 256, s, views);
+    case VMAP_VOXEL_F32: return launch_stage<V>(fuse_kernel<V, VMAP_VOXEL_F32>, grid, 256, s, views);
+    case VMAP_VOXEL_F16: return launch_stage<V>(fuse_kernel<V, VMAP_VOXEL_F16>, grid, 256, s, views);
+    case VMAP_VOXEL_I16: return launch_stage<V>(fuse_kernel<V, VMAP_VOXEL_I16>, grid, 256, s, views);
     default: return cudaErrorInvalidValue;
     }
 }

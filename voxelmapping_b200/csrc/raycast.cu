@@ -105,13 +105,13 @@ __global__ void __launch_bounds__(256) phong_kernel(const float4* vmap, size_t v
 template <class V>
 cudaError_t launch_zrange(const V& views, const Launcher& l, cudaStream_t s)
 {
-    return launch_stage(zrange_kernel<V>, stage_grid(l, l.zrange), 256, s, views);
+    return launch_stage<V>(zrange_kernel<V>, stage_grid(l, l.zrange), 256, s, views);
 }
 
 template <class V>
 cudaError_t launch_normals(const V& views, int totalTiles, const Launcher& l, cudaStream_t s)
 {
-    return launch_stage(normals_kernel<V>, stage_grid(l, l.normals, totalTiles), 256, s, views);
+    return launch_stage<V>(normals_kernel<V>, stage_grid(l, l.normals, totalTiles), 256, s, views);
 }
 
 template cudaError_t launch_zrange<OneView>(const OneView&, const Launcher&, cudaStream_t);

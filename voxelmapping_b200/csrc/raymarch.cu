@@ -85,7 +85,7 @@ static cudaError_t raycast_persistent(const V& views, const Launcher& l, cudaStr
     const int fit = occ[threads == 256];
     // CTAs beyond those resident would only start once others finish: cap at occupancy
     const int per_sm = l.raycast > 0 && l.raycast < fit ? l.raycast : fit;
-    return launch_stage(raycast_kernel<V, FMT>, stage_grid(l, per_sm), threads, s, views, l.tileOrder, l.tileW);
+    return launch_stage<V>(raycast_kernel<V, FMT>, stage_grid(l, per_sm), threads, s, views, l.tileOrder, l.tileW);
 }
 
 template <class V>

@@ -197,10 +197,10 @@ __device__ __forceinline__ bool block_visible(int bx, int by, int bz, const Xf& 
 }
 
 // ------------------------------------------------ programmatic dependent launch
-// The per-frame stage kernels are launched with programmatic stream
-// serialization (launch_stage): a stage's CTAs may be scheduled while the
-// previous kernel on the stream drains, hiding the launch between dependent
-// stages. Every stage kernel calls stage_entry() first, before it reads or
+// A single map's per-frame stage kernels are launched with programmatic
+// stream serialization (launch_stage): a stage's CTAs may be scheduled while
+// the previous kernel on the stream drains, hiding the launch between
+// dependent stages. Every stage kernel calls stage_entry() first, before it reads or
 // writes anything: griddepcontrol.wait returns once the previous kernel has
 // completed and its writes are visible (at once for a launch without a
 // programmatic dependency), and launch_dependents then lets the next stage be
