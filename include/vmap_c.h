@@ -251,6 +251,15 @@ vmap_status vmap_batch_destroy(vmap_batch* batch);
 /* frames: n_maps entries. Asynchronous on `stream`; may block only until the
  * step before last has copied its descriptors. */
 vmap_status vmap_batch_step(vmap_batch* batch, const vmap_batch_frame* frames, void* stream);
+/* Test of the persistent step's bounded wait (no counterpart in the
+ * reference): stages `frames` as vmap_batch_step does, then runs the step as
+ * the persistent launch with one task-ring entry reserved and never written,
+ * so no warp can take work. After stall_ms (1 .. 10000) without progress every
+ * warp raises VMAP_FLAG_STEP_STALLED in every map of the batch and the launch
+ * ends; the maps are left mid-step (reset them). Asynchronous on `stream`;
+ * never captured into the batch's graphs. */
+vmap_status vmap_batch_stall_probe(vmap_batch* batch, const vmap_batch_frame* frames, uint32_t stall_ms,
+                                   void* stream);
 
 /* ---- launch shapes (no counterpart in the reference, which hard-codes its
  * grids). Every stage's grid in CTAs per SM; each kernel strides over its work

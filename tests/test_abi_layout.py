@@ -154,6 +154,11 @@ def test_every_entry_point_refuses_null_and_bad_sizes_without_a_device():
         "vmap_batch_set_map": lambda: lib.vmap_batch_set_map(None, 0, None),
         "vmap_batch_destroy": lambda: lib.vmap_batch_destroy(None),
         "vmap_batch_step": lambda: lib.vmap_batch_step(None, None, None),
+        # (a non-NULL batch with a stall limit out of range is refused before it is read)
+        "vmap_batch_stall_probe": lambda: (lib.vmap_batch_stall_probe(None, None, 100, None),
+                                           lib.vmap_batch_stall_probe(C.c_void_p(1), (L.BatchFrame * 1)(), 0, None),
+                                           lib.vmap_batch_stall_probe(C.c_void_p(1), (L.BatchFrame * 1)(), 10001,
+                                                                      None)),
         "vmap_get_launch_config": lambda: lib.vmap_get_launch_config(None, None),
         "vmap_set_launch_config": lambda: lib.vmap_set_launch_config(None, None),
         "vmap_batch_get_launch_config": lambda: lib.vmap_batch_get_launch_config(None, None),

@@ -390,3 +390,55 @@ def test_persistent_step_equals_stage_launches_on_many_maps():
         assert a.stats()["error_flags"] == c.stats()["error_flags"] == 0, i
     for b in batches.values():
         b.release()
+
+
+def test_persistent_step_wait_is_bounded():
+    """The persistent step's waits end on their own. With one task-ring entry
+    that nothing writes (vmap_batch_stall_probe), every warp gives up once the
+    stall limit passes without progress: the launch ends, every map carries
+    VMAP_FLAG_STEP_STALLED, and the context stays usable (the reset maps then
+    step normally and equal single-map calls)."""
+    import time
+    wls = workloads()[:2]
+    scenes = [synth.Scene(wl) for wl in wls]
+    maps = [make_map(wl) for wl in wls]
+    solo = [make_map(wl) for wl in wls]
+    batch = MapBatch(maps)
+    batch.set_launch_config(batch_schedule=2)
+    side = torch.cuda.Stream()
+
+    def frame(step):
+        fr = [sc.render(step) for sc in scenes]
+        depths = [torch.from_numpy(d.view(np.int16)).cuda() for d, _, _ in fr]
+        rgbs = [torch.from_numpy(c).cuda().reshape(wl.height, -1) if wl.with_color else None
+                for (_, c, _), wl in zip(fr, wls)]
+        vb = [torch.full((wl.height, wl.width, 4), 7.0, device="cuda") for wl in wls]
+        return depths, rgbs, [p for _, _, p in fr], vb
+
+    depths, rgbs, poses, vb = frame(0)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    with torch.cuda.stream(side):
+        batch.stall_probe(depths, rgbs, poses, vb, stall_ms=200)
+    side.synchronize()
+    dt = time.perf_counter() - t0
+    assert 0.15 < dt < 10.0, dt
+    for m in maps:
+        assert m.stats()["error_flags"] & L.FLAG_STEP_STALLED
+        m.clear_errors()
+        m.reset()
+    depths, rgbs, poses, vb = frame(3)
+    torch.cuda.synchronize()
+    with torch.cuda.stream(side):
+        batch.step(depths, rgbs, poses, vb)
+    side.synchronize()
+    for i, (wl, vm) in enumerate(zip(wls, solo)):
+        if wl.with_color:
+            vm.FuseDepthAndImage(rgbs[i], depths[i], poses[i])
+        else:
+            vm.FuseDepth(depths[i], poses[i])
+        v = vm.RenderScene(None, poses[i])
+        torch.cuda.synchronize()
+        assert np.array_equal(np.nan_to_num(v.cpu().numpy(), nan=-9.0), np.nan_to_num(vb[i].cpu().numpy(), nan=-9.0))
+        assert maps[i].stats()["error_flags"] == 0
+    batch.release()

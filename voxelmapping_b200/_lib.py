@@ -110,6 +110,7 @@ SIGNATURES = {
     "vmap_batch_create": (C.c_int, [C.POINTER(P), C.c_int, C.POINTER(P)]),
     "vmap_batch_destroy": (C.c_int, [P]),
     "vmap_batch_step": (C.c_int, [P, C.POINTER(BatchFrame), P]),
+    "vmap_batch_stall_probe": (C.c_int, [P, C.POINTER(BatchFrame), C.c_uint32, P]),
     "vmap_get_stats": (C.c_int, [P, P, C.POINTER(Stats)]),
     "vmap_clear_errors": (C.c_int, [P, P]),
     "vmap_export_blocks": (C.c_int, [P, P, P, P, P, C.c_uint32, C.POINTER(C.c_uint32), P]),

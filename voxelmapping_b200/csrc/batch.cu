@@ -219,14 +219,16 @@ vmap_status vmap_batch_destroy(vmap_batch* b)
     return VMAP_OK;
 }
 
-vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void* stream)
+}  // extern "C"
+
+namespace {
+
+// Validates the step's frames and writes their descriptors into staging
+// buffer `buf` (after the copy out of it, recorded in the step before last,
+// has run).
+vmap_status stage_frames(vmap_batch* b, const vmap_batch_frame* frames, cudaStream_t s, int buf)
 {
-    if (!b || !frames) return VMAP_ERR_INVALID_ARG;
-    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
     const int n = (int)b->maps.size();
-    const int buf = b->next;
-    // the staging buffer is reused every other step: wait until the copy out
-    // of it (recorded in the step before last) has run
     if (b->eventUsed[buf]) VMAP_BCK(cudaEventSynchronize(b->copied[buf]));
     for (int i = 0; i < n; ++i) {
         const vmap_batch_frame& f = frames[i];
@@ -276,6 +278,21 @@ vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void*
         v.out.npitch = np;
         if (render) VMAP_BCK(next_epoch(m, s, &v.out.epoch));
     }
+    return VMAP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void* stream)
+{
+    if (!b || !frames) return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int n = (int)b->maps.size();
+    const int buf = b->next;
+    const vmap_status st = stage_frames(b, frames, s, buf);
+    if (st != VMAP_OK) return st;
     const size_t bytes = sizeof(MapView) * (size_t)n;
     if (s == nullptr) {  // the legacy stream cannot be captured: launch directly
         VMAP_BCK(cudaMemcpyAsync(b->dViews[buf], b->hViews[buf], bytes, cudaMemcpyHostToDevice, s));
@@ -302,6 +319,23 @@ vmap_status vmap_batch_step(vmap_batch* b, const vmap_batch_frame* frames, void*
         }
         VMAP_BCK(cudaGraphLaunch(b->exec[buf], s));
     }
+    b->eventUsed[buf] = true;
+    b->next = buf ^ 1;
+    return VMAP_OK;
+}
+
+vmap_status vmap_batch_stall_probe(vmap_batch* b, const vmap_batch_frame* frames, uint32_t stall_ms, void* stream)
+{
+    if (!b || !frames || stall_ms == 0 || stall_ms > 10000) return VMAP_ERR_INVALID_ARG;
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const int buf = b->next;
+    const vmap_status st = stage_frames(b, frames, s, buf);
+    if (st != VMAP_OK) return st;
+    ManyViews mv{b->dViews[buf], (int)b->maps.size(), b->dQueue};
+    VMAP_BCK(cudaMemcpyAsync(b->dViews[buf], b->hViews[buf], sizeof(MapView) * b->maps.size(),
+                             cudaMemcpyHostToDevice, s));
+    VMAP_BCK(cudaEventRecord(b->copied[buf], s));
+    VMAP_BCK(launch_step(mv, b->dSched, b->fmt, b->launcher, s, 1000000ull * stall_ms, true));
     b->eventUsed[buf] = true;
     b->next = buf ^ 1;
     return VMAP_OK;

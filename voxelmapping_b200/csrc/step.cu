@@ -42,7 +42,6 @@ constexpr int kWarpSet = 256;                         // one warp's staged block
 constexpr int kVisGroups = 4;   // visibility: 4 groups of 32 blocks
 constexpr int kFuseBlocks = 4;  // fusion: 4 visible blocks
 constexpr int kZTasks = 128;    // z-range: 128 link / fold tasks
-constexpr unsigned long long kStallNs = 2000000000ull;  // wait without progress before giving up
 
 __device__ __forceinline__ unsigned vload(const unsigned* p) { return *(volatile const unsigned*)p; }
 __device__ __forceinline__ int vload(const int* p) { return *(volatile const int*)p; }
@@ -99,7 +98,7 @@ struct Grab {
 
 // Lane 0: the next item, from the oldest ring entry with items left; task -1
 // when every map is finished or the wait stalled.
-__device__ Grab grab(const ManyViews& views, StepSched* S, unsigned& h)
+__device__ Grab grab(const ManyViews& views, StepSched* S, unsigned& h, unsigned long long stallNs)
 {
     const unsigned nmaps = (unsigned)views.count();
     unsigned seenTail = ~0u, seenDone = ~0u, sleep = 32;
@@ -130,7 +129,7 @@ __device__ Grab grab(const ManyViews& views, StepSched* S, unsigned& h)
             seenTail = tail;
             seenDone = done;
             since = global_ns();
-        } else if (global_ns() - since > kStallNs) {
+        } else if (global_ns() - since > stallNs) {
             for (unsigned i = 0; i < nmaps; ++i)
                 if (views[i].m.ctr) atomicOr(views[i].m.ctr + C_ERR, VMAP_FLAG_STEP_STALLED);
             return Grab{-1, 0, 0, 0};
@@ -142,7 +141,7 @@ __device__ Grab grab(const ManyViews& views, StepSched* S, unsigned& h)
 
 template <int FMT>
 __global__ void __launch_bounds__(256, 4) step_kernel(const __grid_constant__ ManyViews views, StepSched* S,
-                                                       int order, int tw)
+                                                       int order, int tw, unsigned long long stallNs)
 {
     __shared__ unsigned long long s_wkey[8][kWarpCache];
     __shared__ int s_wslot[8][kWarpCache];
@@ -193,7 +192,7 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const __grid_constant__ Ma
             }
             if (lane == 0) {
                 unsigned h = (unsigned)st[H];
-                const Grab g = grab(views, S, h);
+                const Grab g = grab(views, S, h, stallNs);
                 st[H] = (int)h;
                 st[CUR] = g.task;
                 st[TOTAL] = g.total;
@@ -269,7 +268,8 @@ __global__ void __launch_bounds__(256, 4) step_kernel(const __grid_constant__ Ma
 }
 
 template <int FMT>
-cudaError_t launch_step_fmt(const ManyViews& views, StepSched* S, const Launcher& l, cudaStream_t s)
+cudaError_t launch_step_fmt(const ManyViews& views, StepSched* S, const Launcher& l, cudaStream_t s,
+                            unsigned long long stallNs, bool reserveUnwritten)
 {
     // resident CTAs per SM (a static initialiser runs once, thread-safely)
     static const int fit = [] {
@@ -281,19 +281,24 @@ cudaError_t launch_step_fmt(const ManyViews& views, StepSched* S, const Launcher
     const int per_sm = l.raycast > 0 && l.raycast < fit ? l.raycast : fit;
     cudaError_t e = cudaMemsetAsync(S, 0, sizeof(StepSched), s);
     if (e != cudaSuccess) return e;
-    step_kernel<FMT><<<stage_grid(l, per_sm), 256, 0, s>>>(views, S, l.tileOrder, l.tileW);
+    if (reserveUnwritten) {  // tail = 1 with ring[0] left 0
+        static const unsigned one = 1u;
+        if ((e = cudaMemcpyAsync(&S->tail, &one, sizeof one, cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+    }
+    step_kernel<FMT><<<stage_grid(l, per_sm), 256, 0, s>>>(views, S, l.tileOrder, l.tileW, stallNs);
     return cudaGetLastError();
 }
 
 }  // namespace
 
-cudaError_t launch_step(const ManyViews& views, StepSched* S, int fmt, const Launcher& l, cudaStream_t s)
+cudaError_t launch_step(const ManyViews& views, StepSched* S, int fmt, const Launcher& l, cudaStream_t s,
+                        unsigned long long stallNs, bool reserveUnwritten)
 {
     switch (fmt) {
-    case VMAP_VOXEL_REF: return launch_step_fmt<VMAP_VOXEL_REF>(views, S, l, s);
-    case VMAP_VOXEL_F32: return launch_step_fmt<VMAP_VOXEL_F32>(views, S, l, s);
-    case VMAP_VOXEL_F16: return launch_step_fmt<VMAP_VOXEL_F16>(views, S, l, s);
-    case VMAP_VOXEL_I16: return launch_step_fmt<VMAP_VOXEL_I16>(views, S, l, s);
+    case VMAP_VOXEL_REF: return launch_step_fmt<VMAP_VOXEL_REF>(views, S, l, s, stallNs, reserveUnwritten);
+    case VMAP_VOXEL_F32: return launch_step_fmt<VMAP_VOXEL_F32>(views, S, l, s, stallNs, reserveUnwritten);
+    case VMAP_VOXEL_F16: return launch_step_fmt<VMAP_VOXEL_F16>(views, S, l, s, stallNs, reserveUnwritten);
+    case VMAP_VOXEL_I16: return launch_step_fmt<VMAP_VOXEL_I16>(views, S, l, s, stallNs, reserveUnwritten);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -29,7 +29,14 @@ struct StepSched {
     StepTask task[kMaxBatch * ST_COUNT];  // task id = map * ST_COUNT + stage
 };
 
+// A warp that waits this long without progress gives up (VMAP_FLAG_STEP_STALLED).
+constexpr unsigned long long kStepStallNs = 2000000000ull;
+
 // Clears S and runs one step of every map in `views` as one persistent launch.
-cudaError_t launch_step(const ManyViews& views, StepSched* S, int fmt, const Launcher& l, cudaStream_t s);
+// With reserveUnwritten, ring entry 0 is reserved but never written, so the
+// step cannot proceed: every warp waits on it until stallNs pass without
+// progress (the test of the bounded wait).
+cudaError_t launch_step(const ManyViews& views, StepSched* S, int fmt, const Launcher& l, cudaStream_t s,
+                        unsigned long long stallNs = kStepStallNs, bool reserveUnwritten = false);
 
 }  // namespace vmapb

@@ -380,6 +380,16 @@ class MapBatch:
         """One fuse + render step over every map of the batch. ``depths[i]`` None
         skips map i's fusion and ``vmaps[i]`` None its render (a fuse-only or
         render-only request); both None leave the map idle."""
+        s = self._fill(depths, rgbs, poses, vmaps, nmaps, depth_scale, stream)
+        L.check(self._lib.vmap_batch_step(self._h, self._frames, s), "vmap_batch_step")
+
+    def stall_probe(self, depths, rgbs, poses, vmaps, nmaps=None, stall_ms=200, depth_scale=0.001, stream=None):
+        """vmap_batch_stall_probe: the step as one persistent launch that cannot
+        proceed, so its bounded wait runs out after stall_ms."""
+        s = self._fill(depths, rgbs, poses, vmaps, nmaps, depth_scale, stream)
+        L.check(self._lib.vmap_batch_stall_probe(self._h, self._frames, int(stall_ms), s), "vmap_batch_stall_probe")
+
+    def _fill(self, depths, rgbs, poses, vmaps, nmaps, depth_scale, stream):
         import torch
         for i, m in enumerate(self.maps):
             f = self._frames[i]
@@ -400,5 +410,4 @@ class MapBatch:
             n = nmaps[i] if nmaps is not None else None
             f.nmap_dev = n.data_ptr() if n is not None else None
             f.nmap_pitch = n.stride(0) * 4 if n is not None else 0
-        s = C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
-        L.check(self._lib.vmap_batch_step(self._h, self._frames, s), "vmap_batch_step")
+        return C.c_void_p(stream if stream is not None else torch.cuda.current_stream().cuda_stream)
