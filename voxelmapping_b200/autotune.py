@@ -4,13 +4,13 @@ The library's kernels stride over their work items, so a stage's grid (CTAs
 per SM, vmap_launch_config) changes only its time. The tuner measures the
 candidates on the caller's own data and keeps the fastest:
 
-* a single map (`tune_map`): every trial sets every stage to one candidate and
-  reads the per-stage CUDA-event times (vmap_timing_*), so all stages are
-  tuned together; candidates are visited round-robin several times and each
-  keeps its median; then the ray marcher's own parameters, which share the
-  stage's time with its grid, one after another with the rest fixed at their
-  best: the tile shape (width 8, 16 or 4 of a 32-ray tile), threads per CTA
-  (256 or 128) and the tile order;
+* a single map (`tune_map`): coordinate descent on whole-step time, every
+  stage's grid and then the ray marcher's tile shape (width 8, 16 or 4 of a
+  32-ray tile), threads per CTA (256 or 128) and tile order, one field at a
+  time with the rest fixed at their best; a field's candidates are visited
+  round-robin several times and each keeps its median. Per-stage events would
+  serialise the stage launches that programmatic dependent launch overlaps,
+  so only whole steps are timed;
 * a batch (`tune_batch`): the stages run inside one recorded CUDA graph, so
   the whole step is timed, one stage at a time (coordinate descent);
 * the mesh grid (`tune_mesh`): the counting pass of vmap_polygonize.
@@ -99,66 +99,38 @@ def store(key, config, meta=None):
 
 
 def tune_map(vm, step, n_steps, rounds=3, warmup=3):
-    """Tunes a single map's stage grids. step(i) runs step i (fuse + render)
-    on the current stream. Returns (best config, {field: {candidate: median ms}})."""
+    """Tunes a single map's launch shapes by coordinate descent on whole-step
+    time (CUDA events around n_steps steps, no per-stage events: those
+    serialise the stage launches that programmatic dependent launch lets
+    overlap). step(i) runs step i (fuse + render) on the current stream; every
+    field's candidates are measured in interleaved rounds, so they see the same
+    stretch of frames. Returns (best config, {field: {candidate: median ms per
+    step}})."""
     import torch
-    lib = L.lib()
-    base = vm.get_launch_config()
+    best = vm.get_launch_config()
     for i in range(warmup):
         step(i)
     torch.cuda.synchronize()
-    n_cand = max(len(CANDIDATES[f]) for f in STAGE)
-    samples = {f: {c: [] for c in CANDIDATES[f]} for f in STAGE}
     it = warmup
-    for _ in range(rounds):
-        for t in range(n_cand):
-            cfg = dict(base)
-            for f in STAGE:
-                cfg[f] = CANDIDATES[f][t % len(CANDIDATES[f])]
-            vm.set_launch_config(**cfg)
-            L.check(lib.vmap_timing_enable(vm._map, 8 * n_steps))
-            for _ in range(n_steps):
-                step(it)
-                it += 1
-            torch.cuda.synchronize()
-            ms = (C.c_double * 7)()
-            cnt = (C.c_uint32 * 7)()
-            L.check(lib.vmap_timing_read(vm._map, ms, cnt))
-            L.check(lib.vmap_timing_enable(vm._map, 0))
-            for f, stage in STAGE.items():
-                i = L.STAGES.index(stage)
-                if cnt[i]:
-                    samples[f][cfg[f]].append(ms[i] / cnt[i])
-    best = dict(base)
     table = {}
-    for f in STAGE:
-        med = {c: statistics.median(v) for c, v in samples[f].items() if v}
-        if med:  # a stage the step never runs (a render without normals) keeps its shape
-            table[f] = med
-            best[f] = min(med, key=med.get)
-    # the ray marcher's tile shape, threads per CTA and tile order, one at a
-    # time with the other shapes fixed at their best
-    i = L.STAGES.index("raycast")
-    for f in RAYCAST_PARAMS:
-        times = {c: [] for c in CANDIDATES[f]}
+    for f in list(STAGE) + RAYCAST_PARAMS:
+        samples = {c: [] for c in CANDIDATES[f]}
         for _ in range(rounds):
-            for c in times:
+            for c in samples:
                 vm.set_launch_config(**dict(best, **{f: c}))
-                L.check(lib.vmap_timing_enable(vm._map, 8 * n_steps))
+                step(it)  # the first step after a change of shape is not timed
+                it += 1
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()
                 for _ in range(n_steps):
                     step(it)
                     it += 1
+                b.record()
                 torch.cuda.synchronize()
-                ms = (C.c_double * 7)()
-                cnt = (C.c_uint32 * 7)()
-                L.check(lib.vmap_timing_read(vm._map, ms, cnt))
-                L.check(lib.vmap_timing_enable(vm._map, 0))
-                if cnt[i]:
-                    times[c].append(ms[i] / cnt[i])
-        med = {c: statistics.median(v) for c, v in times.items() if v}
-        if med:
-            table[f] = med
-            best[f] = min(med, key=med.get)
+                samples[c].append(a.elapsed_time(b) / n_steps)
+        med = {c: statistics.median(v) for c, v in samples.items()}
+        table[f] = med
+        best[f] = min(med, key=med.get)
     vm.set_launch_config(**best)
     return best, table
 
