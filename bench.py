@@ -677,12 +677,19 @@ def run_product(args):
         tmp = VoxelMapping(wl.width, wl.height, wl.K, voxel_format=wl.voxel_format, with_color=wl.with_color,
                            max_weight=wl.max_weight)
         tmp.CreateMap(wl.num_entries, wl.num_blocks, wl.voxel_size)
-
-        def tstep(i):
-            j = i % nfr
+        # every trial fuses and renders the same frame after the same prefix,
+        # so the candidates are compared on one workload (the blocks a frame
+        # sees and its rays do not change when it is fused again)
+        for j in range(P0):
             L.check(lib.vmap_fuse_depth_rgb(tmp._map, depth_d[j].data_ptr(), L.DEPTH_U16, wl.width * 2,
                                             wl.depth_scale, rgb_d[j].data_ptr(), wl.width * 3, poses[j], sp))
-            L.check(lib.vmap_render_scene(tmp._map, poses[j], vmap.data_ptr(), vpitch, nmap.data_ptr(), vpitch, sp))
+        j0 = P0
+
+        def tstep(i):
+            L.check(lib.vmap_fuse_depth_rgb(tmp._map, depth_d[j0].data_ptr(), L.DEPTH_U16, wl.width * 2,
+                                            wl.depth_scale, rgb_d[j0].data_ptr(), wl.width * 3, poses[j0], sp))
+            L.check(lib.vmap_render_scene(tmp._map, poses[j0], vmap.data_ptr(), vpitch, nmap.data_ptr(), vpitch,
+                                          sp))
         best, table = AT.tune_map(tmp, tstep, n_steps=8)
         best["mesh_ctas_per_sm"], table["mesh_ctas_per_sm"] = AT.tune_mesh(tmp)
         tmp.release()
