@@ -140,7 +140,7 @@ vmap_status vmap_batch_create(vmap_map* const* maps, int n_maps, vmap_batch** ou
                 return VMAP_ERR_INVALID_ARG;
             }
         b->maps.push_back(maps[i]);
-        b->totalAllocTiles += tiles_32x8(c.width, c.height);
+        b->totalAllocTiles += stage_tiles(c.width, c.height);
     }
     b->totalNormalTiles = b->totalAllocTiles;
     return finish_create(b, out);

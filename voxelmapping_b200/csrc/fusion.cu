@@ -12,7 +12,8 @@
 namespace vmapb {
 
 // ---------------------------------------------------------------- allocation
-// A 256-thread CTA per 32x8-pixel tile, one thread per depth pixel. The
+// A 256-thread CTA per 32 x kStageTileH-pixel tile, kStageTileH / 8 depth
+// pixels per thread. The
 // samples of a pixel's band are walked without touching global memory: each
 // block a pixel enters is staged in a CTA-wide shared-memory set, and once
 // the whole tile has been walked its distinct blocks (a few dozen) are
@@ -31,7 +32,7 @@ __global__ void __launch_bounds__(256, 8) alloc_kernel(V views)
     __shared__ int pre[kMaxBatch + 1];
     __shared__ unsigned long long set[kTileSet];
     for (int i = threadIdx.x; i < kTileSet; i += blockDim.x) set[i] = kEmptyKey;
-    map_prefix(views, [](const MapView& v) { return alloc_tiles(v); }, pre);  // ends with __syncthreads
+    map_prefix(views, [](const MapView& v) { return alloc_tiles<kStageTileH>(v); }, pre);  // ends with __syncthreads
     const int nmaps = views.count();
     if (blockIdx.x == 0)
         for (int i = threadIdx.x; i < nmaps; i += blockDim.x)
@@ -44,9 +45,14 @@ __global__ void __launch_bounds__(256, 8) alloc_kernel(V views)
         const int t = item - pre[mi];
         const int tx = (v.cam.W + 31) >> 5;
         const int x = (t % tx) * 32 + (threadIdx.x & 31);
-        const int y = (t / tx) * 8 + (threadIdx.x >> 5);
-        if (x < v.cam.W && y < v.cam.H)
-            band_blocks(v, x, y, [&](unsigned long long key, int bx, int by, int bz) {
+        const int y0 = (t / tx) * kStageTileH + (threadIdx.x >> 5);
+        float d[kStageTileH / 8];  // this thread's pixels (x, y0 + 8 r), depths loaded first
+#pragma unroll
+        for (int r = 0; r < kStageTileH / 8; ++r)
+            d[r] = x < v.cam.W && y0 + 8 * r < v.cam.H ? read_depth(v.in, x, y0 + 8 * r) : __int_as_float(0x7fffffff);
+#pragma unroll 1
+        for (int r = 0; r < kStageTileH / 8; ++r)
+            band_blocks_at(v, x, y0 + 8 * r, d[r], [&](unsigned long long key, int bx, int by, int bz) {
                 stage_block<kTileSet>(set, m, key, bx, by, bz);
             });
         __syncthreads();

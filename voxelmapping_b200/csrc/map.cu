@@ -547,7 +547,7 @@ static vmap_status fuse_impl(vmap_map* m, const void* depth, int dtype, size_t d
     ov.v.in.rgb = rgb;
     ov.v.in.rgbPitch = rgbPitch;
     ov.queue = m->dm.ctr + C_RAYQ;
-    const int tiles = tiles_32x8(m->cfg.width, m->cfg.height);
+    const int tiles = stage_tiles(m->cfg.width, m->cfg.height);
     // alloc_kernel clears the visible counter the visibility kernel fills
     VMAP_CK(staged(m, VMAP_STAGE_ALLOC, s, [&] { return launch_alloc(ov, tiles, m->launcher, s); }));
     VMAP_CK(staged(m, VMAP_STAGE_VISIBILITY, s, [&] { return launch_visibility(ov, m->launcher, s); }));
@@ -623,7 +623,7 @@ vmap_status vmap_render_scene(vmap_map* m, const double pose[16], float* vmap_de
     VMAP_CK(staged(m, VMAP_STAGE_RAYCAST, s, [&] { return launch_raycast(ov, m->cfg.voxel_format, m->launcher, s); }));
     if (nmap_dev)
         VMAP_CK(staged(m, VMAP_STAGE_NORMALS, s, [&] {
-            return launch_normals(ov, tiles_32x8(m->cfg.width, m->cfg.height), m->launcher, s);
+            return launch_normals(ov, stage_tiles(m->cfg.width, m->cfg.height), m->launcher, s);
         }));
     return VMAP_OK;
 }
@@ -737,7 +737,7 @@ vmap_status vmap_compute_normal(const float* vmap_dev, size_t vmap_pitch, float*
     VMAP_CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     Launcher l;
     l.numSMs = sms;
-    VMAP_CK(launch_normals(ov, tiles_32x8(width, height), l, as_stream(stream)));
+    VMAP_CK(launch_normals(ov, stage_tiles(width, height), l, as_stream(stream)));
     return VMAP_OK;
 }
 

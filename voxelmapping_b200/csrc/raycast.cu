@@ -52,13 +52,14 @@ __global__ void __launch_bounds__(256) zrange_kernel(V views)
 }
 
 // ------------------------------------------------------------------ normals
-// One 256-thread CTA per 32x8-pixel tile.
+// One 256-thread CTA per 32 x kStageTileH-pixel tile, kStageTileH / 8 pixels
+// per thread.
 template <class V>
 __global__ void __launch_bounds__(256) normals_kernel(V views)
 {
     stage_entry();
     __shared__ int pre[kMaxBatch + 1];
-    map_prefix(views, [](const MapView& v) { return normal_tiles(v); }, pre);
+    map_prefix(views, [](const MapView& v) { return normal_tiles<kStageTileH>(v); }, pre);
     const int nmaps = views.count();
     const int total = pre[nmaps];
     for (int item = blockIdx.x; item < total; item += gridDim.x) {
@@ -66,7 +67,9 @@ __global__ void __launch_bounds__(256) normals_kernel(V views)
         const MapView& v = views[mi];
         const int t = item - pre[mi];
         const int tx = (v.cam.W + 31) >> 5;
-        normal_pixel<true>(v, (t % tx) * 32 + (threadIdx.x & 31), (t / tx) * 8 + (threadIdx.x >> 5));
+        const int x = (t % tx) * 32 + (threadIdx.x & 31), y0 = (t / tx) * kStageTileH + (threadIdx.x >> 5);
+#pragma unroll
+        for (int r = 0; r < kStageTileH / 8; ++r) normal_pixel<true>(v, x, y0 + 8 * r);
     }
 }
 

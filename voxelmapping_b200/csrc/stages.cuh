@@ -36,10 +36,12 @@ __device__ __forceinline__ float read_depth(const FrameIn& f, int x, int y)
 }
 
 // ---------------------------------------------------------------- allocation
-// Maps without fusion work this step (no frame) contribute no items.
+// 32 x TH-pixel tiles of a map's frame; maps without fusion work this step
+// (no frame) contribute none.
+template <int TH>
 __device__ __forceinline__ int alloc_tiles(const MapView& v)
 {
-    return v.in.active ? ((v.cam.W + 31) >> 5) * ((v.cam.H + 7) >> 3) : 0;
+    return v.in.active ? ((v.cam.W + 31) >> 5) * ((v.cam.H + TH - 1) / TH) : 0;
 }
 
 constexpr int ilog2(int n) { return n > 1 ? 1 + ilog2(n >> 1) : 0; }
@@ -366,11 +368,12 @@ __device__ __forceinline__ void zrange_block(const MapView& v, int slot)
 // ------------------------------------------------------------------ normals
 // computeNormalKernel: normalize((v[x+1] - v[x-1]) x (v[y+1] - v[y-1])),
 // w = 1. Undefined pixels (last row / column, NaN neighbour) are written
-// all-NaN. Work is split into 32x8-pixel tiles of every map that wants a
+// all-NaN. Work is split into 32-pixel-wide tiles of every map that wants a
 // normal map.
+template <int TH>
 __device__ __forceinline__ int normal_tiles(const MapView& v)
 {
-    return v.out.nmap ? ((v.cam.W + 31) >> 5) * ((v.cam.H + 7) >> 3) : 0;
+    return v.out.nmap ? ((v.cam.W + 31) >> 5) * ((v.cam.H + TH - 1) / TH) : 0;
 }
 
 template <bool NC>

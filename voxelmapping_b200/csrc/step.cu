@@ -57,12 +57,12 @@ __device__ __forceinline__ unsigned long long global_ns()
 __device__ __forceinline__ int stage_items(const MapView& v, int s, int tw)
 {
     switch (s) {
-    case ST_ALLOC: return alloc_tiles(v);
+    case ST_ALLOC: return alloc_tiles<8>(v);
     case ST_VISIBLE: return v.in.active ? (allocated_blocks(v.m) + 32 * kVisGroups - 1) / (32 * kVisGroups) : 0;
     case ST_FUSE: return v.in.active ? ((int)vload(v.m.ctr + C_VISIBLE) + kFuseBlocks - 1) / kFuseBlocks : 0;
     case ST_ZRANGE: return (links_pending(v) + zrange_blocks(v) + kZTasks - 1) / kZTasks;
     case ST_RAYCAST: return ray_tiles(v, tw);
-    default: return normal_tiles(v);
+    default: return normal_tiles<8>(v);
     }
 }
 
