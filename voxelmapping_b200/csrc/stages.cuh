@@ -171,11 +171,11 @@ __device__ __forceinline__ void visibility_group(const MapView& v, int g, int la
 // ----------------------------------------------------------------- fusion
 // DepthFusionFunctor / ImageFusionFunctor for the NV (4 or 8) consecutive
 // voxels v0 .. v0 + NV - 1 of an x-row of block `slot` (one vector of NV
-// voxel words, one NV-byte word per colour plane). Every load is issued as
-// early as its address is known, so a thread waits on two memory round trips
-// rather than four: the voxel words and colour planes before the projections,
-// each projected pixel's depth and colour right after its projection. Nothing
-// is written unless one of the 4 voxels updates.
+// voxel words, one NV-byte word per colour plane). The projections come
+// first: each projected pixel's depth and colour are loaded right after its
+// projection, and the group's voxel words and colour planes only when one of
+// its voxels updates, so groups behind the surface or outside the frame move
+// no voxel bytes. Nothing is written unless a voxel updates.
 template <int FMT, bool COLOR, int DT, int NV = 4>
 __device__ __forceinline__ void fuse_block(const MapView& v, int slot, int v0)
 {
@@ -188,13 +188,8 @@ __device__ __forceinline__ void fuse_block(const MapView& v, int slot, int v0)
     Word* blk = L::words_rw(m, slot);
     static_assert(NV == 4 || NV == 8, "4 or 8 voxels of an x-row");
     Word w[NV];
-    load_vec<NV * sizeof(Word)>(blk + v0, w);
     unsigned char c[3][NV];
     unsigned char* crow = reinterpret_cast<unsigned char*>(blk) + L::kRgbOff + v0;
-    if constexpr (COLOR) {
-#pragma unroll
-        for (int k = 0; k < 3; ++k) load_vec<NV>(crow + k * kBlockVoxels, c[k]);
-    }
     const int vx0 = bp.x * 8 + lx0;
     const float wy = __fmul_rn(__int2float_rn(bp.y * 8 + ly), m.vs);
     const float wz = __fmul_rn(__int2float_rn(bp.z * 8 + lz), m.vs);
@@ -222,6 +217,11 @@ __device__ __forceinline__ void fuse_block(const MapView& v, int slot, int v0)
         mask |= 1u << x;
     }
     if (!mask) return;
+    load_vec<NV * sizeof(Word)>(blk + v0, w);
+    if constexpr (COLOR) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) load_vec<NV>(crow + k * kBlockVoxels, c[k]);
+    }
 #pragma unroll
     for (int x = 0; x < NV; ++x) {
         if (!(mask & (1u << x))) continue;
