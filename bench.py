@@ -200,6 +200,31 @@ def gpu_index(local_rank):
     return local_rank
 
 
+def bind_to_gpu_cpus(local_rank):
+    """Restricts this process to the CPUs NVML reports as local to the rank's
+    GPU (its NUMA node), so pinned host buffers and the threads that drive the
+    copies sit next to the GPU's PCIe link, as a deployment would place them.
+    Returns the previous CPU set (to restore for host-only work), or None when
+    NVML gives no affinity."""
+    try:
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            h = pynvml.nvmlDeviceGetHandleByUUID(str(gpu_index(local_rank)))
+            words = pynvml.nvmlDeviceGetCpuAffinity(h, (os.cpu_count() + 63) // 64)
+        finally:
+            pynvml.nvmlShutdown()
+        cpus = {64 * i + b for i, w in enumerate(words) for b in range(64) if (int(w) >> b) & 1}
+        before = os.sched_getaffinity(0)
+        cpus &= before
+        if not cpus or cpus == before:
+            return None
+        os.sched_setaffinity(0, cpus)
+        return before
+    except Exception:
+        return None
+
+
 # -------------------------------------------------------------- CPU baseline
 def cpu_oracle_run(wl, frames, n_threads, seconds=None, steps=None, om=None, precision=0, counts=None):
     """Reference algorithm (the oracle in FP32 reference arithmetic, or FP64,
@@ -411,6 +436,7 @@ def run_reference(args):
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": "frames/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     try:
+        bind_to_gpu_cpus(0)  # as the product arm: host threads and pinned buffers next to the GPU
         line["reference_cuda_build"] = reference_cuda_build(args, wl, frames)
     except Exception as e:  # reported, not fatal: the CPU port is the arm's value
         line["reference_cuda_build"] = {"unavailable": "failed: %s" % e}
@@ -630,6 +656,7 @@ def run_product(args):
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300))
     torch.cuda.set_device(local)
+    host_cpus = bind_to_gpu_cpus(local)  # the full CPU set, restored for the CPU baseline
     dev = torch.device("cuda", local)
     wl = synth.WORKLOADS[WORKLOAD]
     import dataclasses
@@ -771,6 +798,10 @@ def run_product(args):
             "launch_config": launch_cfg, "tuning": tune_src,
             "map": {"allocated_blocks": int(st["allocated_blocks"]), "visible_blocks_mean": float(vis_timed.mean()),
                     "visible_blocks_mean_stage_pass": float(vis.mean()), "error_flags": int(st["error_flags"])}}
+    line["config"]["host_cpus"] = (
+        "the %d CPUs local to the GPU (NVML affinity) for the GPU arms, all %d for the CPU baseline"
+        % (len(os.sched_getaffinity(0)), len(host_cpus)) if host_cpus else
+        "all host CPUs (NVML reports no narrower affinity for the GPU)")
 
     # --- mesh: marching cubes over every allocated block of the map -------
     # (Polygonize, marching_cubes.cu:251-305): a counting pass, then the emit
@@ -895,8 +926,12 @@ def run_product(args):
 
     # --- CPU baseline: oracle on the host cores (rank 0, N = 1 only) -------
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        if host_cpus:  # the CPU leg gets every host core
+            os.sched_setaffinity(0, host_cpus)
         threads = os.cpu_count() or 1
         cb = cpu_baseline(wl, scene, frames, threads, seconds=args.cpu_seconds, prefix=args.prefix)
+        if host_cpus:
+            bind_to_gpu_cpus(local)
         cb["sample"] = ("frames %d..%d of %s after %d untimed prefix frames (fuse + raycast + normals each, FP32 "
                         "reference-algorithm restatement, %d threads; FP64 beside)"
                         % (args.prefix, args.prefix + cb["frames_timed"] - 1, WORKLOAD, args.prefix, threads))
