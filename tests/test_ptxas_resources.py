@@ -30,6 +30,10 @@ def test_ray_marcher_fits_four_ctas_per_sm(report):
         # the neighbour-link trilinear path spills up to ~300 B at 64 registers;
         # measured as fast as 3 CTAs/SM without the register cap
         assert r["registers"] <= 64 and r["spill_stores"] <= 320, (k, r)
+        # the FP32 and FP16 words (formats 1, 2): the loop head keeps only the
+        # sample's voxel live across the warp's block lookup, so little spills
+        if ", 1>" in k or ", 2>" in k:
+            assert r["spill_stores"] <= 64, (k, r)
 
 
 def test_persistent_step_fits_four_ctas_per_sm(report):

@@ -86,6 +86,23 @@ struct March {
         }
     };
 
+    // The voxel floor(p) of a sample: all the loop head needs (the block
+    // lookup and the first read). The trilinear fractions and far corners are
+    // computed from the same position only on the samples that interpolate,
+    // so they are not live across the warp's block lookup.
+    struct Cell {
+        int x0, y0, z0;
+    };
+
+    static __device__ __forceinline__ Cell cell(float3 p)
+    {
+        Cell c;
+        c.x0 = __float2int_rz(floorf(p.x));
+        c.y0 = __float2int_rz(floorf(p.y));
+        c.z0 = __float2int_rz(floorf(p.z));
+        return c;
+    }
+
     static __device__ __forceinline__ Corners corners(float3 p)
     {
         Corners c;
@@ -258,7 +275,7 @@ struct March {
     // First half of a loop iteration: the key of the block the sample at res
     // falls in when that block is not the ray's current one and not its
     // cached neighbour (kEmptyKey otherwise: no lookup needed).
-    static __device__ __forceinline__ unsigned long long lookup_key(Ray& r, const Corners& c)
+    static __device__ __forceinline__ unsigned long long lookup_key(Ray& r, const Cell& c)
     {
         const int bx = vox2blk(c.x0), by = vox2blk(c.y0), bz = vox2blk(c.z0);
         if (bx == r.cbx && by == r.cby && bz == r.cbz) return kEmptyKey;
@@ -278,7 +295,7 @@ struct March {
 
     // Second half: one iteration of the reference loop with the sample's block
     // (r.cblk) known; true when the ray leaves the loop.
-    static __device__ __forceinline__ bool advance(const MapView& v, Ray& r, const Corners& c)
+    static __device__ __forceinline__ bool advance(const MapView& v, Ray& r, const Cell& p)
     {
         const DevMap& m = v.m;
         const int bx = r.cbx, by = r.cby, bz = r.cbz;
@@ -289,9 +306,10 @@ struct March {
             return false;
         }
         bool valid;
-        float sdf = voxel(m, r.cblk, c.x0, c.y0, c.z0, valid);  // read_sdf at floor(res)
+        float sdf = voxel(m, r.cblk, p.x0, p.y0, p.z0, valid);  // read_sdf at floor(res)
         if (sdf <= 0.5f && sdf >= -0.5f) {
             float s[8];
+            const Corners c = corners(r.res);  // c.x0 == p.x0 (same position)
             if (c.inner()) {
                 // corner 0 is the sample just read; the other 7 are independent
                 // loads (loading all 8 with every sample was measured slower)
@@ -400,7 +418,7 @@ __device__ __forceinline__ void march_tile(const MapView& v, int mi, int q, int 
                                            unsigned long long* wkey, int* wslot, int lane)
 {
     typedef March<FMT, NC> M;
-    typedef typename M::Corners Corners;
+    typedef typename M::Cell Cell;
     const unsigned full = 0xffffffffu;
     // the map's q-th tile in the requested order (row-major tile index t):
     // 0 bottom rows first, 1 top rows first, 2 alternating from both ends
@@ -414,12 +432,12 @@ __device__ __forceinline__ void march_tile(const MapView& v, int mi, int q, int 
     // iteration; finished lanes idle until the tile is done, then all
     // finish together
     while (__ballot_sync(full, live)) {
-        Corners c;
+        Cell c;
         unsigned long long key = kEmptyKey;
         if (live) {
             if (!(r.dist_s < r.dist_lim)) live = false;
             else {
-                c = M::corners(r.res);
+                c = M::cell(r.res);
                 key = M::lookup_key(r, c);
             }
         }
