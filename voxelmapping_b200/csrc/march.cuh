@@ -274,16 +274,25 @@ struct March {
 
     // First half of a loop iteration: the key of the block the sample at res
     // falls in when that block is not the ray's current one and not its
-    // cached neighbour (kEmptyKey otherwise: no lookup needed).
+    // cached second block (kEmptyKey otherwise: no lookup needed). The block
+    // the ray leaves becomes the cached second block: the refinement step
+    // after the zero crossing steps back by up to half a truncation band and
+    // often lands in it.
     static __device__ __forceinline__ unsigned long long lookup_key(Ray& r, const Cell& c)
     {
         const int bx = vox2blk(c.x0), by = vox2blk(c.y0), bz = vox2blk(c.z0);
         if (bx == r.cbx && by == r.cby && bz == r.cbz) return kEmptyKey;
+        const bool second = bx == r.obx && by == r.oby && bz == r.obz;
+        const int oblk = r.oblk;
+        r.obx = r.cbx;
+        r.oby = r.cby;
+        r.obz = r.cbz;
+        r.oblk = r.cblk;
         r.cbx = bx;
         r.cby = by;
         r.cbz = bz;
-        if (bx == r.obx && by == r.oby && bz == r.obz) {
-            r.cblk = r.oblk;
+        if (second) {
+            r.cblk = oblk;
             return kEmptyKey;
         }
         if (!coord_ok(bx, by, bz)) {
@@ -340,18 +349,27 @@ struct March {
     }
 
     // After the loop: two refinement steps when the zero crossing was found
-    // (ray_tracing.cu:381-393), then the camera-frame vertex or a miss.
+    // (ray_tracing.cu:381-393), then the camera-frame vertex or a miss. The
+    // first step is taken here; the block of the interpolation's first corner
+    // becomes the ray's current block, and its key is returned when it is
+    // neither the block the ray is in nor the one it came from (the step back
+    // lands in one of those on most rays) and has to be looked up.
+    static __device__ __forceinline__ unsigned long long refine_key(const MapView& v, Ray& r)
+    {
+        if (!(r.sdf <= 0.f)) return kEmptyKey;
+        r.res = fma3(__fmul_rn(r.sdf, v.out.rts), r.dir, r.res);
+        return lookup_key(r, cell(r.res));
+    }
+
+    // The rest, with the current block's slot (r.cblk) known.
     static __device__ __forceinline__ void finish(const MapView& v, Ray& r)
     {
         const RenderOut& o = v.out;
         bool found = false;
         if (r.sdf <= 0.f) {
-            float stp = __fmul_rn(r.sdf, o.rts);
-            r.res = fma3(stp, r.dir, r.res);
             bool valid;
-            const float s = interp(v.m, r, r.res, valid);
-            stp = __fmul_rn(s, o.rts);
-            r.res = fma3(stp, r.dir, r.res);
+            const float s = interp(v.m, r, r.res, valid);  // first corner's block: r.cblk
+            r.res = fma3(__fmul_rn(s, o.rts), r.dir, r.res);
             found = valid;
         }
         float4 out;
@@ -445,7 +463,17 @@ __device__ __forceinline__ void march_tile(const MapView& v, int mi, int q, int 
         if (key != kEmptyKey) r.cblk = slot;
         if (live && M::advance(v, r, c)) live = false;
     }
-    if (started) M::finish(v, r);
+    // the first refinement step's block, looked up per lane when the ray's
+    // two cached blocks miss it (measured faster than a warp-cache lookup
+    // here, which makes every lane of the tile wait for the slowest)
+    if (started) {
+        const unsigned long long key = M::refine_key(v, r);
+        if (key != kEmptyKey) {
+            const int3 b = unpack_key(key);
+            r.cblk = hash_find<NC>(v.m, b.x, b.y, b.z);
+        }
+        M::finish(v, r);
+    }
 }
 
 // Empty the warp's block cache (all lanes of the warp).
