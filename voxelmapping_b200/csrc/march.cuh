@@ -464,8 +464,8 @@ __device__ __forceinline__ void march_tile(const MapView& v, int mi, int q, int 
         if (live && M::advance(v, r, c)) live = false;
     }
     // the first refinement step's block, looked up per lane when the ray's
-    // two cached blocks miss it (measured faster than a warp-cache lookup
-    // here, which makes every lane of the tile wait for the slowest)
+    // two cached blocks miss it (measured faster on the batched step than the
+    // same lookup through the warp's block cache)
     if (started) {
         const unsigned long long key = M::refine_key(v, r);
         if (key != kEmptyKey) {
