@@ -1,6 +1,6 @@
 """bench.py's host-side bookkeeping without a GPU: the clock record taken from
-nvidia-smi samples (busy samples only, throttle reasons by name), percentiles
-and the whole-job throughput."""
+nvidia-smi samples (busy samples only, throttle reasons by name), percentiles,
+the whole-job throughput and the L2 flush buffer."""
 import sys
 from pathlib import Path
 
@@ -42,3 +42,15 @@ def test_throughput_and_percentiles():
     assert bench.job_throughput(200, 100.0, 4) == pytest.approx(4 * 200 / 0.1)
     assert bench.percentile([1.0, 2.0, 3.0, 4.0], 50) == pytest.approx(2.5)
     assert bench.percentile([], 99) == 0.0
+
+
+def test_l2_flush_buffer_exceeds_l2_and_fills_with_16_byte_vectors():
+    """The flush writes FLUSH_BYTES (twice the 126 MB L2) as float32, the dtype
+    whose fill_ stores 16 bytes per thread; a uint8 buffer of the same size
+    fills at about half the speed, which the pipelined e2e run would count."""
+    import torch
+    buf = bench.l2_flush_buffer(torch.device("cpu"))
+    assert buf.dtype == torch.float32
+    assert buf.numel() * buf.element_size() == bench.FLUSH_BYTES >= 2 * 126 * 10**6
+    buf.fill_(7 & 255)
+    assert float(buf[-1]) == 7.0
